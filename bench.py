@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 phase-retrieval backend on its headline workload.
+
+Workload: 256 x 256 complex64, 32 starts, recipe
+``repeat(10, RAAR(50, 0.9), Shrinkwrap(0.3, 1.0)), ER(200)`` (700 iterations),
+on the seeded ``gaussians`` problem (5 Gaussians in a disk, ramp + filtered
+noise phase, Poisson 1e6, beamstop r = 8, autocorrelation support). One step
+is one run of the whole recipe over all 32 starts; the metric is
+start-iterations per second (starts x iterations / time).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own 32 starts on its own GPU (independent
+replicas, weak scaling); rank 0 prints one JSON line. ``--impl reference``
+times the reference's CPU implementation of the same recipe on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "iterations/s per 256² start, batched vs plain, at <=1e-5 rel err; HBM GB/s"
+UNIT = "start-iterations/s"
+SHAPE = (256, 256)
+STARTS = 32
+SEED = 1000
+WORKLOAD = "gaussians 256x256 complex64, 32 starts, repeat(10, RAAR(50,0.9), Shrinkwrap(0.3,1.0)), ER(200)"
+# Algorithmic bytes per element of each line pass (SURVEY 8d figures applied to
+# what each fused pass must move): modulus pass reads the wave and the FP32
+# amplitude and writes the wave; update pass reads the wave, support and old
+# iterate and writes the iterate and the next wave.
+PASS_BYTES = {"modulus (y-axis fwd+P_M+inv)": 8 + 4 + 8, "update (x-axis inv+update+fwd)": 8 + 1 + 8 + 8 + 8}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        peaks = json.loads(path.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch_update:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(f"/tmp/qpb_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.path.open("w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, value in zip(names, parts[5:9]):
+                if value.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_sample(problem_arrays, starts, iterations, threads):
+    """Times `iterations` RAAR iterations of `starts` starts on the host CPU with
+    the reference's own CpuSolver (compiled from its sources) when available,
+    else the oracle's numpy/pocketfft port. Returns (seconds, kind, label)."""
+    intensity, mask = problem_arrays
+    from oracle import ref as oracle_ref
+
+    if oracle_ref.available():
+        seconds = oracle_ref.time_iterations(intensity, mask, starts, iterations, threads)
+        return seconds, "reference", "QoraPhaseCU CpuSolver (OpenMP loops, project FFT shim)"
+    import numpy as np
+
+    from oracle import fp64
+
+    problem = fp64.make_problem(intensity, None, mask)
+    solver = fp64.Solver(problem, starts=starts, dtype=np.complex64, fft="scipy", workers=threads)
+    t0 = time.perf_counter()
+    solver.run([fp64.op("raar", iterations, 0.9)])
+    return time.perf_counter() - t0, "port", "numpy port of CpuSolver::iterate, scipy.fft (pocketfft)"
+
+
+def cpu_baseline(intensity, mask, budget_s=10.0):
+    threads = len(os.sched_getaffinity(0))
+    iters = 2
+    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads)
+    # grow the sample to about `budget_s` of CPU work
+    iters = max(2, min(200, int(iters * budget_s / max(seconds, 1e-3))))
+    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads)
+    return {
+        "value": STARTS * iters / seconds,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": kind,
+        "sample": f"{STARTS} starts x {iters} RAAR iterations at 256x256 ({label}), {seconds:.1f} s",
+    }
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from qoraphasecu_b200 import workloads
+
+    _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
+    for _ in range(args.warmup):
+        pass  # the sample itself warms up (first call builds FFT plans)
+    samples = []
+    for _ in range(args.steps):
+        samples.append(cpu_baseline(intensity, mask, budget_s=args.cpu_seconds))
+    value = statistics.median(s["value"] for s in samples)
+    base = samples[-1]
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * STARTS * 700 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded gaussians generator)",
+        "config": {"workload": WORKLOAD, "l2": "n/a (host CPU)"},
+        "cpu_baseline": {**base, "value": value},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------- our arm
+def main(argv=None):
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--sync-every", type=int, default=50)
+    parser.add_argument("--cpu-seconds", type=float, default=10.0)
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
+    args = parser.parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    qpc.api.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
+    recipe = workloads.gaussians_recipe()
+    iters = recipe.iterations()
+    stream = torch.cuda.current_stream()
+    problem = qpc.make_problem(intensity, mask=mask)
+    solver = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+                        device=local, stream=stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        solver.run(recipe)
+    barrier()
+
+    step_ms = []
+    launches0 = qpc.kernel_launches()
+    t_wall = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flushed between steps (outside the step events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.run(recipe)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        barrier()
+    wall_s = time.perf_counter() - t_wall
+    launches = qpc.kernel_launches() - launches0
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * STARTS * iters * args.steps / (total_ms / 1e3)
+
+    # Per-pass device time (direct launches between events on the same stream).
+    pass_ms = solver.profile_passes(20)
+    elems = STARTS * SHAPE[0] * SHAPE[1]
+    passes = []
+    for (name, bpe), ms in zip(PASS_BYTES.items(), pass_ms):
+        passes.append({"pass": name, "ms": ms, "bytes": bpe * elems, "gbs": bpe * elems / (ms * 1e6)})
+    dominant = max(passes, key=lambda p: p["ms"])
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic()
+    roofline = {
+        "bound": "hbm",
+        "kernel": dominant["pass"],
+        "achieved": dominant["gbs"],
+        "peak": peak,
+        "peak_source": f"{peak_kind} hbm_gbs",
+        "unit": "GB/s",
+        "frac": dominant["gbs"] / peak,
+        "traffic": traffic,
+        "passes": passes,
+        "note": "32 starts x 256^2 (16 MiB iterate) stay L2-resident across an iteration",
+    }
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded gaussians generator, seed 1000; random starts seed = rank)",
+        "config": {
+            "workload": WORKLOAD,
+            "shape": list(SHAPE),
+            "starts_per_gpu": STARTS,
+            "iterations": iters,
+            "variant": "batched, graph-captured",
+            "sync_every": args.sync_every,
+            "parallelism": f"replicas x{world}",
+            "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write, outside step events)",
+        },
+        "gpu_launches": launches,
+        "wall_s_timed_region": wall_s,
+        "roofline": roofline,
+    }
+
+    if not args.no_extras:
+        # Plain per-start path (the in-repo baseline), one step.
+        plain = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+                           variant="plain", device=local, stream=stream.cuda_stream)
+        plain.run(recipe)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plain.run(recipe)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1))
+        plain.close()
+        plain_value = world * STARTS * iters / (plain_ms / 1e3)
+        # FP16 amplitude storage, same schedule.
+        half = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+                          amp_storage="f16", device=local, stream=stream.cuda_stream)
+        half.run(recipe)
+        barrier()
+        e0.record(stream)
+        half.run(recipe)
+        e1.record(stream)
+        e1.synchronize()
+        half_ms = max_over_ranks(e0.elapsed_time(e1))
+        half.close()
+        line["variants"] = {
+            "plain_per_start": {"value": plain_value, "ms_per_step": plain_ms},
+            "batched_over_plain": value / plain_value,
+            "f16_amplitude": {"value": world * STARTS * iters / (half_ms / 1e3), "ms_per_step": half_ms},
+        }
+
+        # End to end through the public API with host buffers: intensity from
+        # pinned memory in, objects/supports/errors out, every step.
+        pinned = torch.empty(intensity.shape, dtype=torch.float32, pin_memory=True)
+        pinned.numpy()[...] = intensity
+        host_in = pinned.numpy()
+        times = []
+        for k in range(args.warmup + args.steps):
+            barrier()
+            t0 = time.perf_counter()
+            ens = qpc.reconstruct(host_in, mask=mask, recipe=recipe, starts=STARTS, seed=rank,
+                                  sync_every=args.sync_every)
+            times.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(statistics.median(times[args.warmup:]))
+        n = SHAPE[0] * SHAPE[1]
+        line["e2e"] = {
+            "value": world * STARTS * iters / e2e_s,
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(n * (4 + 8 + 4 + 1 + 4)),
+            "d2h_bytes_per_step": int(n * 8 + STARTS * n * (8 + 1) + STARTS * iters * 8),
+            "seconds_per_step": e2e_s,
+            "path": "qoraphasecu_b200.reconstruct (make_problem + solver + results)",
+        }
+        del ens
+
+    line["clocks"] = clocks.summary()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(intensity, mask, budget_s=args.cpu_seconds)
+    solver.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

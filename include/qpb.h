@@ -1,0 +1,167 @@
+/* qpb.h -- C ABI of the B200 phase-retrieval backend (libqpb.so).
+ *
+ * The backend is a new implementation of QoraPhaseCU's qpcu::Solver
+ * (include/qoraphasecu/solver.hpp:67-74 in the reference), selected by a new
+ * qpcu::Backend value. Everything crosses this boundary as plain pointers and
+ * sizes; no C++ exception crosses it. Every function returns a qpb_status;
+ * qpb_last_error() gives the message of the last failure on the calling thread.
+ *
+ * Arrays are centre-origin (index n/2 along each axis is q = 0 or r = 0), as in
+ * the reference's public API (include/qoraphasecu/problem.hpp:24-31). Complex
+ * arrays are interleaved complex64 (re, im float pairs).
+ */
+#ifndef QPB_H_
+#define QPB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. QPB_INVALID_ARGUMENT is the reference's std::invalid_argument
+ * (src/core/solver.cpp:62-78, recipe.cpp:30-61, problem.cpp:21-56);
+ * QPB_RUNTIME_ERROR its std::runtime_error (src/cuda/common.cuh:15-31). */
+typedef enum qpb_status {
+  QPB_OK = 0,
+  QPB_INVALID_ARGUMENT = 1,
+  QPB_RUNTIME_ERROR = 2,
+  QPB_TIMEOUT = 3
+} qpb_status;
+
+/* Storage type of the amplitude (FP32 arithmetic either way). */
+typedef enum qpb_amp_storage { QPB_AMP_F32 = 0, QPB_AMP_F16 = 1, QPB_AMP_BF16 = 2 } qpb_amp_storage;
+
+/* Execution schedule. BATCHED runs `batch` starts per launch with iterations
+ * replayed from CUDA graphs; PLAIN runs one start per launch, launched
+ * directly (the in-repo baseline). Replaces qpcu::Variant (solver.hpp:21-29). */
+typedef enum qpb_variant { QPB_VARIANT_BATCHED = 0, QPB_VARIANT_PLAIN = 1 } qpb_variant;
+
+/* A made problem: the fields of qpcu::Problem (problem.hpp:26-31). */
+typedef struct qpb_problem {
+  int ndim;                /* 2 or 3 */
+  int64_t shape[3];        /* slowest axis first */
+  const float* amplitude;  /* numel, sqrt(clip(intensity, 0)) */
+  const uint8_t* mask;     /* numel, 1 = unusable pixel; NULL = every pixel usable */
+  const uint8_t* support;  /* numel, 1 = inside the object */
+} qpb_problem;
+
+/* qpcu::Options (solver.hpp:40-55) minus the backend and progress fields. */
+typedef struct qpb_options {
+  int starts;              /* >= 1 */
+  int batch;               /* starts per launch, must divide starts; 0 = all */
+  uint64_t seed;           /* seed of the random starting phases */
+  const float* start;      /* starts * numel complex64 centre-origin objects, or NULL */
+  int sync_every;          /* iterations per graph launch and progress interval, >= 1 */
+  int variant;             /* qpb_variant */
+  int amp_storage;         /* qpb_amp_storage */
+  int device;              /* CUDA device ordinal; -1 = the calling thread's current device */
+  void* stream;            /* cudaStream_t the solver enqueues on; NULL = a stream of its own */
+} qpb_options;
+
+/* One recipe operation: the POD form of qpcu::Op (recipe.hpp:44), the same
+ * seven fields as the reference's Python op tuple (python/bindings.cpp:22-23). */
+typedef enum qpb_op_kind {
+  QPB_OP_ER = 0,
+  QPB_OP_HIO = 1,
+  QPB_OP_RAAR = 2,
+  QPB_OP_SHRINKWRAP = 3,
+  QPB_OP_DETWIN_BEGIN = 4,
+  QPB_OP_DETWIN_END = 5
+} qpb_op_kind;
+
+typedef struct qpb_op {
+  int kind;        /* qpb_op_kind */
+  int n;           /* iterations (ER, HIO, RAAR) */
+  float beta;      /* HIO, RAAR */
+  float threshold; /* Shrinkwrap */
+  float sigma;     /* Shrinkwrap */
+  int method;      /* Shrinkwrap: 0 max, 1 rms (qpcu::Threshold, recipe.hpp:25) */
+  int axis;        /* DetwinBegin */
+} qpb_op;
+
+typedef struct qpb_solver qpb_solver;
+
+/* Called every sync_every iterations with the iteration count so far and the
+ * latest Fourier error of each start (qpcu::Progress, solver.hpp:36-38). */
+typedef void (*qpb_progress_fn)(void* user, int iteration, const float* errors, int count);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* qpb_last_error(void);
+
+/* 1 when a CUDA device is present (qpcu::cuda_available, solver.hpp:85). */
+int qpb_cuda_available(void);
+
+/* Selects the device that calls without a solver (make_problem, the single
+ * operators) use on the calling thread. No counterpart in the reference, which
+ * always uses the current device (src/cuda/kernels.cu:15-24). */
+qpb_status qpb_set_device(int device);
+
+/* Replaces qpcu::cuda_device_info (solver.hpp:87-98). name_out holds name_len bytes. */
+qpb_status qpb_device_info(char* name_out, size_t name_len, int* sm_major, int* sm_minor,
+                           size_t* memory_bytes, size_t* l2_bytes, double* peak_bandwidth_gbs);
+
+/* qpcu::make_problem (problem.hpp:35-37, problem.cpp:40-70): validates the
+ * inputs, amplitude = sqrt(max(I, 0)); a NULL support is replaced by the
+ * autocorrelation support at `support_threshold`. Outputs are numel each. */
+qpb_status qpb_make_problem(const float* intensity, int ndim, const int64_t* shape,
+                            const uint8_t* support, const uint8_t* mask, float support_threshold,
+                            float* amplitude_out, uint8_t* mask_out, uint8_t* support_out);
+
+/* qpcu::autocorrelation_support (problem.hpp:42-43, problem.cpp:72-88). */
+qpb_status qpb_autocorrelation_support(const float* intensity, int ndim, const int64_t* shape,
+                                       float threshold, uint8_t* out);
+
+/* qpcu::half_support (problem.hpp:51-52, problem.cpp:101-127), on the device. */
+qpb_status qpb_half_support(const uint8_t* support, int ndim, const int64_t* shape, int axis,
+                            uint8_t* out);
+
+/* qpcu::make_solver for the new backend (solver.cpp:61-86 ->
+ * detail::make_cuda_solver, backends.hpp:9-10): uploads the problem and draws
+ * the starts. */
+qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out);
+
+/* qpcu::Solver::run (solver.hpp:72): validates and runs the recipe, continuing
+ * from the current state; appends one error per iteration to every start. */
+qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);
+
+/* Progress callback (Options::progress, solver.hpp:52-54); NULL disables it. */
+qpb_status qpb_set_progress(qpb_solver* solver, qpb_progress_fn fn, void* user);
+
+/* Iterations run so far (the length of every start's error history). */
+qpb_status qpb_error_count(const qpb_solver* solver, size_t* count);
+qpb_status qpb_starts(const qpb_solver* solver, int* starts);
+
+/* qpcu::Solver::results (solver.hpp:73) into caller buffers: objects
+ * starts * numel complex64, supports starts * numel, errors starts * error_count.
+ * Any output may be NULL. */
+qpb_status qpb_results(qpb_solver* solver, float* objects, uint8_t* supports, float* errors);
+
+void qpb_destroy(qpb_solver* solver);
+
+/* Kernels this library has launched in this process; a replayed CUDA graph
+ * counts each kernel node. No counterpart in the reference: it backs the
+ * launch count that bench.py reports. */
+uint64_t qpb_kernel_launches(void);
+
+/* Runs `iterations` more iterations with every line pass launched directly
+ * between CUDA events on the solver's stream; ms_out[p] receives the mean
+ * duration of pass p of one iteration (2D: modulus pass, update pass; 3D adds
+ * the y-axis inverse and forward passes) and *n_passes their count (<= 8).
+ * Advances the iterate. No counterpart in the reference: it feeds the
+ * per-kernel roofline that bench.py reports. */
+qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
+
+/* Single operators on centre-origin arrays (qpcu::cuda::, operators.hpp:25-33). */
+qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
+                               float* error_out);
+qpb_status qpb_support_project(const uint8_t* support, float* obj, size_t count);
+qpb_status qpb_gaussian_blur(const float* image, int ndim, const int64_t* shape, float sigma,
+                             float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QPB_H_ */

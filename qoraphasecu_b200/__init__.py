@@ -1,0 +1,51 @@
+"""QoraPhase B200 backend: iterative phase retrieval as hand-written sm_100a kernels.
+
+Array in, reconstruction out, with the surface of the reference's
+``qoraphasecu`` package::
+
+    import qoraphasecu_b200 as qpc
+    result = qpc.reconstruct(intensity, support=support)
+
+All public arrays are centre-origin, ``mask=True`` marks an unusable pixel and
+``intensity`` is a measured intensity. Every call runs on the GPU through
+``libqpb.so`` (include/qpb.h); there is no CPU path.
+"""
+
+from .api import (
+    Ensemble,
+    Problem,
+    Reconstruction,
+    Solver,
+    autocorrelation_support,
+    best_index,
+    cuda_available,
+    half_support,
+    make_problem,
+    reconstruct,
+)
+from .operators import gaussian_blur, modulus_project, support_project
+from .recipe import ER, HIO, RAAR, Recipe, Shrinkwrap, default_recipe, detwin, repeat
+
+__all__ = [
+    "ER",
+    "HIO",
+    "RAAR",
+    "Ensemble",
+    "Problem",
+    "Recipe",
+    "Reconstruction",
+    "Shrinkwrap",
+    "Solver",
+    "autocorrelation_support",
+    "best_index",
+    "cuda_available",
+    "default_recipe",
+    "detwin",
+    "gaussian_blur",
+    "half_support",
+    "make_problem",
+    "modulus_project",
+    "reconstruct",
+    "repeat",
+    "support_project",
+]

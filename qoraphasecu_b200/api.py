@@ -1,0 +1,370 @@
+"""``reconstruct``: array in, reconstruction out, on the B200 backend.
+
+Mirrors the reference's ``python/qoraphasecu/api.py`` (``reconstruct`` at
+:120-185, ``Reconstruction``/``Ensemble`` at :16-66) and the C++
+``make_problem``/``make_solver``/``Solver::run``/``results`` chain underneath
+(``include/qoraphasecu/solver.hpp:67-80``), all through ``libqpb.so``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+from dataclasses import dataclass
+from typing import Literal
+
+import numpy as np
+
+from . import _lib
+from .recipe import Recipe, default_recipe
+
+NEGATIVE_WARN_FRACTION = 0.01
+
+
+@dataclass(frozen=True)
+class Reconstruction:
+    """One reconstructed object, defined up to a global phase, a translation and a twin."""
+
+    object: np.ndarray
+    support: np.ndarray
+    errors: np.ndarray
+
+    @property
+    def amplitude(self) -> np.ndarray:
+        return np.abs(self.object)
+
+    @property
+    def phase(self) -> np.ndarray:
+        return np.angle(self.object)
+
+    @property
+    def error(self) -> float:
+        """Final Fourier error (NaN before any iteration); the ranking key."""
+        return float(self.errors[-1]) if self.errors.size else float("nan")
+
+
+@dataclass(frozen=True)
+class Ensemble:
+    """The runs of a multi-start reconstruction, not mutually aligned."""
+
+    runs: tuple
+
+    def __len__(self) -> int:
+        return len(self.runs)
+
+    def __iter__(self):
+        return iter(self.runs)
+
+    def __getitem__(self, index):
+        return self.runs[index]
+
+    @property
+    def ranking(self) -> tuple:
+        """Run indices, lowest final error first."""
+        return tuple(sorted(range(len(self.runs)), key=lambda i: self.runs[i].error))
+
+    @property
+    def best(self) -> Reconstruction:
+        return self.runs[best_index(self.runs)]
+
+
+def best_index(runs) -> int:
+    """Index of the run with the lowest final error; a NaN run never displaces a
+    finite one (src/core/solver.cpp:95-103)."""
+    runs = list(runs)
+    if not runs:
+        raise ValueError("no runs")
+    best = 0
+    for i in range(1, len(runs)):
+        e, b = runs[i].error, runs[best].error
+        if e < b or np.isnan(b):
+            best = i
+    return best
+
+
+def cuda_available() -> bool:
+    return bool(_lib.load().qpb_cuda_available())
+
+
+def set_device(device: int) -> None:
+    """Device used on this thread by calls without a solver (make_problem, operators)."""
+    _lib.check(_lib.load().qpb_set_device(device))
+
+
+def kernel_launches() -> int:
+    """Kernels libqpb.so has launched in this process (graph replays count each node)."""
+    return int(_lib.load().qpb_kernel_launches())
+
+
+def _shape(array: np.ndarray):
+    if array.ndim not in (2, 3):
+        raise ValueError(f"intensity must be 2D or 3D, got ndim={array.ndim}")
+    return _lib.shape_arg(array.shape)
+
+
+def autocorrelation_support(intensity, threshold: float = 0.1) -> np.ndarray:
+    """Loose support from the thresholded autocorrelation (device FFT); shrinkwrap tightens it."""
+    intensity = np.ascontiguousarray(intensity, dtype=np.float32)
+    out = np.empty(intensity.shape, np.uint8)
+    lib = _lib.load()
+    _lib.check(lib.qpb_autocorrelation_support(_lib.ptr(intensity), intensity.ndim,
+                                               _shape(intensity), threshold, _lib.ptr(out)))
+    return out.astype(bool)
+
+
+def half_support(support, axis: int = 0) -> np.ndarray:
+    """The support below its centre of mass along ``axis`` (the detwin cut)."""
+    support = np.ascontiguousarray(support, dtype=bool).view(np.uint8)
+    out = np.empty(support.shape, np.uint8)
+    lib = _lib.load()
+    _lib.check(lib.qpb_half_support(_lib.ptr(support), support.ndim, _shape(support), axis,
+                                    _lib.ptr(out)))
+    return out.astype(bool)
+
+
+@dataclass
+class Problem:
+    """Centre-origin amplitude, mask and support (the reference's qpcu::Problem)."""
+
+    amplitude: np.ndarray
+    mask: np.ndarray
+    support: np.ndarray
+
+    @property
+    def shape(self):
+        return self.amplitude.shape
+
+    def _c(self):
+        p = _lib.Problem()
+        p.ndim = self.amplitude.ndim
+        p.shape = _lib.shape_arg(self.amplitude.shape)
+        p.amplitude = self.amplitude.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        p.mask = self.mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        p.support = self.support.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        return p
+
+
+def make_problem(intensity, support=None, mask=None, support_threshold: float = 0.1) -> Problem:
+    """Validates the inputs and derives the amplitude; a missing support is the
+    autocorrelation support (src/core/problem.cpp:40-70)."""
+    intensity = np.ascontiguousarray(intensity, dtype=np.float32)
+    shape = _shape(intensity)
+    support = _flag("support", support, intensity.shape)
+    mask = _flag("mask", mask, intensity.shape)
+    amp = np.empty(intensity.shape, np.float32)
+    m = np.empty(intensity.shape, np.uint8)
+    s = np.empty(intensity.shape, np.uint8)
+    lib = _lib.load()
+    _lib.check(lib.qpb_make_problem(_lib.ptr(intensity), intensity.ndim, shape, _lib.ptr(support),
+                                    _lib.ptr(mask), support_threshold, _lib.ptr(amp),
+                                    _lib.ptr(m), _lib.ptr(s)))
+    return Problem(amp, m, s)
+
+
+def _flag(name, array, shape):
+    if array is None:
+        return None
+    array = np.ascontiguousarray(array, dtype=bool)
+    if array.shape != shape:
+        raise ValueError(f"{name}.shape {array.shape} != intensity.shape {shape}")
+    return array.view(np.uint8)
+
+
+def _start(init, shape, starts):
+    if init is None:
+        return None
+    init = np.asarray(init, dtype=np.complex64)
+    if init.shape == tuple(shape):
+        init = np.broadcast_to(init, (starts, *shape))
+    if init.shape != (starts, *shape):
+        raise ValueError(
+            f"init.shape {init.shape} must be the intensity's {tuple(shape)} or (starts, *shape)"
+        )
+    return np.ascontiguousarray(init)
+
+
+def _ops(recipe):
+    ops = recipe.ops() if hasattr(recipe, "ops") else list(recipe)
+    array = (_lib.Op * max(len(ops), 1))()
+    for i, (kind, n, beta, threshold, sigma, method, axis) in enumerate(ops):
+        if kind not in _lib.OP_KINDS:
+            raise ValueError(f"unknown recipe operation '{kind}'")
+        if method not in _lib.METHODS:
+            raise ValueError(f"method must be 'max' or 'rms', got {method!r}")
+        array[i] = _lib.Op(_lib.OP_KINDS[kind], int(n), float(beta), float(threshold),
+                           float(sigma), _lib.METHODS[method], int(axis))
+    return array, len(ops)
+
+
+class Solver:
+    """A live reconstruction: starts drawn on construction; ``run`` continues
+    from the current state and appends errors (include/qoraphasecu/solver.hpp:67-74)."""
+
+    def __init__(self, problem: Problem, *, starts: int = 1, batch: int | None = None,
+                 seed: int | None = None, init=None, sync_every: int = 10,
+                 variant: Literal["batched", "plain"] = "batched",
+                 amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
+                 device: int = -1, stream: int | None = None):
+        if variant not in _lib.VARIANTS:
+            raise ValueError(f"unknown variant '{variant}' (this backend has 'batched' and 'plain')")
+        if amp_storage not in _lib.AMP_STORAGE:
+            raise ValueError(f"unknown amp_storage '{amp_storage}'")
+        self.problem = problem
+        self.shape = problem.shape
+        start = _start(init, problem.shape, starts)
+        options = _lib.Options()
+        options.starts = starts
+        options.batch = 0 if batch is None else batch
+        options.seed = 0 if seed is None else seed
+        options.start = (start.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+                         if start is not None else None)
+        options.sync_every = sync_every
+        options.variant = _lib.VARIANTS[variant]
+        options.amp_storage = _lib.AMP_STORAGE[amp_storage]
+        options.device = device
+        options.stream = stream
+        self._lib = _lib.load()
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.qpb_create(ctypes.byref(problem._c()), ctypes.byref(options),
+                                        ctypes.byref(handle)))
+        self._handle = handle
+        self._progress = None
+        if progress is not None:
+            self.set_progress(progress)
+
+    def set_progress(self, fn):
+        """``fn(iteration, errors)`` every ``sync_every`` iterations, on this thread."""
+        if fn is None:
+            self._progress = None
+            _lib.check(self._lib.qpb_set_progress(self._handle, _lib.PROGRESS(), None))
+            return
+
+        def trampoline(_user, iteration, errors, count):
+            fn(iteration, np.ctypeslib.as_array(errors, shape=(count,)).copy())
+
+        self._progress = _lib.PROGRESS(trampoline)
+        _lib.check(self._lib.qpb_set_progress(self._handle, self._progress, None))
+
+    def run(self, recipe=None):
+        ops, count = _ops(default_recipe() if recipe is None else recipe)
+        _lib.check(self._lib.qpb_run(self._handle, ops, count))
+
+    def profile_passes(self, iterations: int = 20):
+        """Mean device time (ms) of each line pass of one iteration, timed with
+        CUDA events around direct launches; advances the iterate."""
+        ms = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        _lib.check(self._lib.qpb_profile_passes(self._handle, iterations, ms, ctypes.byref(n)))
+        return [ms[i] for i in range(n.value)]
+
+    @property
+    def starts(self) -> int:
+        n = ctypes.c_int()
+        _lib.check(self._lib.qpb_starts(self._handle, ctypes.byref(n)))
+        return n.value
+
+    def error_count(self) -> int:
+        n = ctypes.c_size_t()
+        _lib.check(self._lib.qpb_error_count(self._handle, ctypes.byref(n)))
+        return n.value
+
+    def results(self):
+        starts = self.starts
+        count = self.error_count()
+        objects = np.empty((starts, *self.shape), np.complex64)
+        supports = np.empty((starts, *self.shape), np.uint8)
+        errors = np.empty((starts, count), np.float32)
+        _lib.check(self._lib.qpb_results(self._handle, _lib.ptr(objects), _lib.ptr(supports),
+                                         _lib.ptr(errors)))
+        return [Reconstruction(objects[s], supports[s].astype(bool), errors[s])
+                for s in range(starts)]
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.qpb_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def reconstruct(
+    intensity,
+    *,
+    support=None,
+    mask=None,
+    recipe=None,
+    starts: int = 1,
+    batch: int | None = None,
+    seed: int | None = None,
+    init=None,
+    support_threshold: float = 0.1,
+    backend: Literal["auto", "b200"] = "auto",
+    variant: Literal["batched", "plain"] = "batched",
+    sync_every: int = 10,
+    amp_storage: Literal["f32", "f16", "bf16"] = "f32",
+    progress=None,
+) -> Reconstruction | Ensemble:
+    """Array in, reconstruction out.
+
+    Args:
+        intensity: measured intensity, centre-origin, 2D or 3D.
+        support: boolean, True inside the object; None derives the
+            autocorrelation support.
+        mask: boolean, True marks unusable pixels.
+        recipe: a :class:`Recipe` (None: :func:`default_recipe`).
+        starts: random starts; more than one returns an :class:`Ensemble`.
+        batch: starts per launch (``variant="batched"``); None puts all in one.
+        seed: seed of the random starting phases; None means 0.
+        init: starting object(s), centre-origin, shape ``shape`` or
+            ``(starts, *shape)``, cut to the support.
+        backend: ``"auto"`` or ``"b200"``; both run this backend, which needs
+            a CUDA device.
+        variant: ``"batched"`` (graph-captured, all starts per launch) or
+            ``"plain"`` (one start per launch).
+        amp_storage: ``"f32"``, ``"f16"`` or ``"bf16"`` storage of the amplitude.
+        progress: ``fn(iteration, errors)`` every ``sync_every`` iterations.
+    """
+    intensity = np.ascontiguousarray(intensity, dtype=np.float32)
+    if intensity.ndim not in (2, 3):
+        raise ValueError(f"intensity must be 2D or 3D, got ndim={intensity.ndim}")
+    negative = float(np.mean(intensity < 0))
+    if negative > NEGATIVE_WARN_FRACTION:
+        warnings.warn(
+            f"{negative:.1%} of intensity pixels are negative and will be clipped to 0; "
+            "consider masking them instead",
+            stacklevel=2,
+        )
+    if backend not in ("auto", "b200"):
+        raise ValueError(
+            f"backend '{backend}' is not provided here; this package is the 'b200' backend"
+        )
+    if recipe is None:
+        recipe = default_recipe()
+    problem = make_problem(intensity, support, mask, support_threshold)
+    with Solver(problem, starts=starts, batch=batch, seed=seed, init=init, sync_every=sync_every,
+                variant=variant, amp_storage=amp_storage, progress=progress) as solver:
+        solver.run(recipe)
+        runs = solver.results()
+    return runs[0] if starts == 1 else Ensemble(tuple(runs))
+
+
+__all__ = [
+    "Ensemble",
+    "Problem",
+    "Recipe",
+    "Reconstruction",
+    "Solver",
+    "autocorrelation_support",
+    "best_index",
+    "cuda_available",
+    "half_support",
+    "make_problem",
+    "reconstruct",
+]

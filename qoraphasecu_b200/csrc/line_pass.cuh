@@ -1,0 +1,86 @@
+// Line passes: batched 1D FFTs along one axis of a stack of FFT-order arrays,
+// each fused with the point-wise step that follows or precedes it in the
+// phase-retrieval iteration.
+//
+// An n-D transform is a sequence of passes, one per axis. Per iteration the
+// solver runs (2D) Mod along y then Upd along x, keeping the invariant that the
+// wave buffer `w` holds the x-axis transform of the iterate between
+// iterations; 3D adds Inv/Fwd passes along y.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "fft_plan.hpp"
+
+namespace qpb {
+
+enum class Mode : int {
+  kFwd,      // w <- FFT(w)
+  kFwdFromX, // w <- FFT(x)
+  kInv,      // w <- IFFT(w)
+  kMod,      // w <- IFFT(P_M FFT(w)) and the Fourier-error numerator per start
+  kUpd,      // P <- IFFT(w); x <- S ? P : a x + b P; w <- FFT(x)
+  kBlur,     // w <- IFFT(g FFT(w)), g = exp(k f^2) / L along this axis
+  kBlurMag,  // as kBlur on (|x|, 0)
+};
+
+enum class AmpStorage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
+
+// Device control block shared by the kernels of one solver. Captured graphs
+// reference it by address, so per-stage values live here instead of in
+// kernel arguments.
+struct Ctrl {
+  double* errs;    // [capacity][starts_total] Fourier-error numerators
+  int capacity;    // rows of errs
+  float a;         // update coefficients of the current stage
+  float b;
+  int* counters;   // iteration counter per start group
+};
+
+// Per-start shrinkwrap level accumulator.
+struct LevelAcc {
+  double sum;
+  unsigned long long count;
+  int max_bits;  // bits of a non-negative float: ordered like the float
+  int pad;
+};
+
+struct PassParams {
+  float2* w;
+  float2* x;
+  const void* amp;                // signed amplitude (-1 masked), FFT order, one per problem
+  const std::uint8_t* support;    // [batch][n]
+  Ctrl* ctrl;
+  LevelAcc* level;                // [batch], kBlur with level != 0
+  const float2* twiddle;          // W_L^k, k < L
+  long long n;                    // elements per start
+  int L;                          // line length
+  int S;                          // element stride of a line
+  int lines;                      // lines in this launch
+  int lines_per_start;
+  int lpc;                        // lines per CTA (divides lines_per_start)
+  int group;                      // counter index (kMod, kUpd)
+  int start0;                     // first global start of the batch (error column)
+  int starts_total;               // error row width
+  int stages;
+  int radix[kMaxStages];
+  float scale;                    // 1/sqrt(n) (kMod)
+  float blur_k;                   // -2 (pi sigma)^2 (kBlur)
+  int level_method;               // 0 none, 1 max, 2 rms (kBlur)
+  float coef_a;                   // immediate coefficients when !coef_from_ctrl
+  float coef_b;
+  int coef_from_ctrl;
+  int bump_counter;               // kUpd increments ctrl->counters[group]
+  AmpStorage amp_storage;
+};
+
+// Launches one generic line pass on `stream`.
+void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream);
+
+// Lines per CTA for a line of length L with `lines_per_start` lines per start.
+int choose_lpc(int L, int S, int lines_per_start);
+
+}  // namespace qpb

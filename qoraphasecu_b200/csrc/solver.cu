@@ -1,0 +1,671 @@
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "solver.hpp"
+
+namespace qpb {
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+// out[i] = in[(i + off(n)) mod n] per axis, src/core/layout.hpp:71-88.
+template <class T>
+std::vector<T> host_roll(const T* in, Dims3 d, bool to_fft_order) {
+  auto off = [&](int len) { return to_fft_order ? len / 2 : len - len / 2; };
+  const int o0 = off(d.d0), o1 = off(d.d1), o2 = off(d.d2);
+  std::vector<T> out(static_cast<std::size_t>(d.n()));
+  std::size_t i = 0;
+  for (int z = 0; z < d.d0; ++z) {
+    const int sz = (z + o0) % d.d0;
+    for (int y = 0; y < d.d1; ++y) {
+      const std::size_t row = (static_cast<std::size_t>(sz) * d.d1 + (y + o1) % d.d1) * d.d2;
+      for (int x = 0; x < d.d2; ++x) out[i++] = in[row + (x + o2) % d.d2];
+    }
+  }
+  return out;
+}
+
+// Signed amplitude (-1 on masked pixels) in the requested storage type.
+std::vector<unsigned char> signed_amplitude(const std::vector<float>& amp,
+                                            const std::vector<std::uint8_t>& mask,
+                                            AmpStorage storage) {
+  const std::size_t n = amp.size();
+  std::vector<unsigned char> out;
+  switch (storage) {
+    case AmpStorage::kF32: {
+      out.resize(n * sizeof(float));
+      auto* p = reinterpret_cast<float*>(out.data());
+      for (std::size_t i = 0; i < n; ++i) p[i] = mask[i] ? -1.0f : amp[i];
+      break;
+    }
+    case AmpStorage::kF16: {
+      out.resize(n * sizeof(__half));
+      auto* p = reinterpret_cast<__half*>(out.data());
+      for (std::size_t i = 0; i < n; ++i) p[i] = __float2half_rn(mask[i] ? -1.0f : amp[i]);
+      break;
+    }
+    case AmpStorage::kBF16: {
+      out.resize(n * sizeof(__nv_bfloat16));
+      auto* p = reinterpret_cast<__nv_bfloat16*>(out.data());
+      for (std::size_t i = 0; i < n; ++i) p[i] = __float2bfloat16_rn(mask[i] ? -1.0f : amp[i]);
+      break;
+    }
+  }
+  return out;
+}
+
+double usable_energy(const std::vector<float>& amp, const std::vector<std::uint8_t>& mask) {
+  double e = 0.0;
+  for (std::size_t i = 0; i < amp.size(); ++i) {
+    if (!mask[i]) e += static_cast<double>(amp[i]) * amp[i];
+  }
+  return e;
+}
+
+template <class T>
+DeviceBuffer<T> upload(const std::vector<T>& host, cudaStream_t s) {
+  DeviceBuffer<T> d(host.size());
+  QPB_CHECK(cudaMemcpyAsync(d.get(), host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  QPB_CHECK(cudaStreamSynchronize(s));
+  return d;
+}
+
+int axis_stride(Dims3 d, int axis3) {
+  return axis3 == 2 ? 1 : axis3 == 1 ? d.d2 : d.d1 * d.d2;
+}
+
+int axis_len(Dims3 d, int axis3) { return axis3 == 0 ? d.d0 : axis3 == 1 ? d.d1 : d.d2; }
+
+}  // namespace
+
+Dims3 dims_of(const ProblemView& p) {
+  if (p.ndim != 2 && p.ndim != 3) {
+    throw InvalidArgument("problem shape must be 2D or 3D, got ndim=" + std::to_string(p.ndim));
+  }
+  for (int a = 0; a < p.ndim; ++a) {
+    if (p.shape[a] < 1) throw InvalidArgument("shape has a zero-length axis");
+    if (p.shape[a] > kMaxLine) {
+      throw InvalidArgument("axis length " + std::to_string(p.shape[a]) +
+                            " exceeds the supported maximum " + std::to_string(kMaxLine));
+    }
+  }
+  if (p.ndim == 2) return {1, static_cast<int>(p.shape[0]), static_cast<int>(p.shape[1])};
+  return {static_cast<int>(p.shape[0]), static_cast<int>(p.shape[1]), static_cast<int>(p.shape[2])};
+}
+
+// src/core/recipe.cpp:30-61, plus the axis check half_support makes (problem.cpp:104-106).
+void validate_recipe(const OpDesc* ops, std::size_t count) {
+  if (count == 0) throw InvalidArgument("recipe is empty");
+  bool in_detwin = false;
+  for (std::size_t i = 0; i < count; ++i) {
+    const OpDesc& o = ops[i];
+    switch (o.kind) {
+      case kOpER:
+        if (o.n < 1) throw InvalidArgument("ER needs n >= 1");
+        break;
+      case kOpHIO:
+        if (o.n < 1) throw InvalidArgument("HIO needs n >= 1");
+        break;
+      case kOpRAAR:
+        if (o.n < 1) throw InvalidArgument("RAAR needs n >= 1");
+        break;
+      case kOpShrinkwrap:
+        if (!(o.threshold > 0.0f) || !(o.sigma >= 0.0f)) {
+          throw InvalidArgument("Shrinkwrap needs threshold > 0, sigma >= 0");
+        }
+        if (o.method != 0 && o.method != 1) throw InvalidArgument("unknown shrinkwrap method");
+        break;
+      case kOpDetwinBegin:
+        if (in_detwin) throw InvalidArgument("nested detwin");
+        in_detwin = true;
+        break;
+      case kOpDetwinEnd:
+        if (!in_detwin) throw InvalidArgument("DetwinEnd without DetwinBegin");
+        in_detwin = false;
+        break;
+      default:
+        throw InvalidArgument("unknown recipe operation " + std::to_string(o.kind));
+    }
+  }
+  if (in_detwin) throw InvalidArgument("DetwinBegin without DetwinEnd");
+}
+
+int recipe_iterations(const OpDesc* ops, std::size_t count) {
+  long long total = 0;
+  for (std::size_t i = 0; i < count; ++i) {
+    if (ops[i].kind == kOpER || ops[i].kind == kOpHIO || ops[i].kind == kOpRAAR) total += ops[i].n;
+  }
+  if (total > (1LL << 30)) throw InvalidArgument("recipe has too many iterations");
+  return static_cast<int>(total);
+}
+
+// ------------------------------------------------------------------ PassRunner
+PassRunner::PassRunner(Dims3 d, int ndim, PlanCache& plans) : d_(d), ndim_(ndim) {
+  for (int a = 0; a < 3; ++a) {
+    plans_[a] = (ndim == 2 && a == 0) ? nullptr : &plans.get(axis_len(d, a));
+  }
+}
+
+PassParams PassRunner::params(Mode mode, int axis3, int batch) const {
+  (void)mode;
+  PassParams p{};
+  const LinePlan& plan = *plans_[axis3];
+  p.n = d_.n();
+  p.L = plan.length;
+  p.S = axis_stride(d_, axis3);
+  p.lines_per_start = static_cast<int>(p.n / p.L);
+  p.lines = batch * p.lines_per_start;
+  p.lpc = choose_lpc(p.L, p.S, p.lines_per_start);
+  p.stages = plan.stages;
+  for (int s = 0; s < plan.stages; ++s) p.radix[s] = plan.radix[s];
+  p.twiddle = plan.twiddle;
+  p.scale = 1.0f / std::sqrt(static_cast<float>(p.n));
+  return p;
+}
+
+void PassRunner::launch(Mode mode, int axis3, PassParams p, cudaStream_t s) const {
+  (void)axis3;
+  launch_line_pass(mode, p, s);
+}
+
+// ---------------------------------------------------------------------- Solver
+Solver::Solver(const ProblemView& problem, const SolverOptions& options)
+    : d_(dims_of(problem)),
+      ndim_(problem.ndim),
+      n_(d_.n()),
+      starts_(options.starts),
+      batch_(1),
+      groups_(1),
+      options_(options),
+      select_(options.device),
+      stream_(options.stream),
+      runner_(d_, ndim_, plans_) {
+  if (options.starts < 1) throw InvalidArgument("starts must be >= 1");
+  if (options.sync_every < 1) throw InvalidArgument("sync_every must be >= 1");
+  if (options.batch < 0 || (options.batch > 0 && options.starts % options.batch != 0)) {
+    throw InvalidArgument("batch must divide starts");
+  }
+  if (!problem.amplitude || !problem.support) {
+    throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
+  }
+  batch_ = options.variant == Variant::kPlain ? 1 : (options.batch ? options.batch : starts_);
+  groups_ = starts_ / batch_;
+  options_.start = nullptr;
+
+  const auto amp = host_roll(problem.amplitude, d_, true);
+  std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
+  if (problem.mask) {
+    mask = host_roll(problem.mask, d_, true);
+    for (auto& m : mask) m = m != 0;
+  }
+  auto sup = host_roll(problem.support, d_, true);
+  for (auto& s : sup) s = s != 0;
+  energy_ = usable_energy(amp, mask);
+  amp_ = upload(signed_amplitude(amp, mask, options.amp_storage), stream_);
+
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  x_ = DeviceBuffer<float2>(total);
+  w_ = DeviceBuffer<float2>(total);
+  support_ = DeviceBuffer<std::uint8_t>(total);
+  saved_ = DeviceBuffer<std::uint8_t>(total);
+  level_ = DeviceBuffer<LevelAcc>(static_cast<std::size_t>(batch_));
+  moments_ = DeviceBuffer<unsigned long long>(2 * static_cast<std::size_t>(starts_));
+  ctrl_ = DeviceBuffer<Ctrl>(1);
+  counters_ = DeviceBuffer<int>(static_cast<std::size_t>(groups_));
+  QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
+  QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
+  const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
+  QPB_CHECK(cudaMemcpyAsync(ctrl_.get(), &ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  QPB_CHECK(cudaMemcpyAsync(support_.get(), sup.data(), sup.size(), cudaMemcpyHostToDevice, stream_));
+  for (int s = 1; s < starts_; ++s) {
+    QPB_CHECK(cudaMemcpyAsync(support_.get() + static_cast<std::size_t>(s) * n_, support_.get(),
+                              static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
+  }
+  errors_.assign(static_cast<std::size_t>(starts_), {});
+
+  if (options.start) {
+    // Given starts, centre-origin: to FFT order, cut to the support (cpu_solver.cpp:37-41).
+    QPB_CHECK(cudaMemcpyAsync(w_.get(), options.start, total * sizeof(float2),
+                              cudaMemcpyHostToDevice, stream_));
+    roll<float2>(w_.get(), x_.get(), d_, starts_, true, stream_);
+    support_project(x_.get(), support_.get(), n_, starts_, stream_);
+    wave_valid_ = false;
+    establish_wave();
+  } else {
+    // Random phases on the measured amplitude, inverse transform, cut to the
+    // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
+    auto amp_f = upload(amp, stream_);
+    for (int g = 0; g < groups_; ++g) {
+      random_wave(w(g), amp_f.get(), n_, batch_, options.seed,
+                  static_cast<std::uint64_t>(g) * batch_, stream_);
+      const int outer = runner_.outer();
+      runner_.launch(Mode::kInv, outer, base(Mode::kInv, outer, g), stream_);
+      if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, base(Mode::kInv, 1, g), stream_);
+      PassParams u = base(Mode::kUpd, 2, g);
+      u.coef_from_ctrl = 0;
+      u.coef_a = 0.0f;
+      u.coef_b = 0.0f;
+      u.bump_counter = 0;
+      runner_.launch(Mode::kUpd, 2, u, stream_);
+      if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+    }
+    stream_.sync();
+    wave_valid_ = true;
+  }
+  stream_.sync();
+}
+
+Solver::~Solver() { cudaStreamSynchronize(stream_); }
+
+PassParams Solver::base(Mode mode, int axis3, int g) const {
+  PassParams p = runner_.params(mode, axis3, batch_);
+  p.w = w(g);
+  p.x = x(g);
+  p.amp = amp_.get();
+  p.support = support(g);
+  p.ctrl = ctrl_.get();
+  p.level = level_.get();
+  p.group = g;
+  p.start0 = g * batch_;
+  p.starts_total = starts_;
+  p.coef_from_ctrl = 1;
+  p.bump_counter = 1;
+  p.amp_storage = options_.amp_storage;
+  return p;
+}
+
+void Solver::enqueue_establish(int g) {
+  runner_.launch(Mode::kFwdFromX, 2, base(Mode::kFwdFromX, 2, g), stream_);
+  if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+}
+
+void Solver::establish_wave() {
+  for (int g = 0; g < groups_; ++g) enqueue_establish(g);
+  wave_valid_ = true;
+}
+
+// One iteration of group g (cpu_solver.cpp:84-89): forward FFT, modulus with
+// the error, inverse FFT, update; the x-axis forward of the new iterate is
+// folded into the update pass.
+void Solver::enqueue_iteration(int g) {
+  const int outer = runner_.outer();
+  runner_.launch(Mode::kMod, outer, base(Mode::kMod, outer, g), stream_);
+  if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, base(Mode::kInv, 1, g), stream_);
+  runner_.launch(Mode::kUpd, 2, base(Mode::kUpd, 2, g), stream_);
+  if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+}
+
+void Solver::run(const OpDesc* ops, std::size_t count) {
+  validate_recipe(ops, count);
+  for (std::size_t i = 0; i < count; ++i) {
+    if (ops[i].kind == kOpDetwinBegin && (ops[i].axis < 0 || ops[i].axis >= ndim_)) {
+      throw InvalidArgument("detwin axis out of range");
+    }
+  }
+  const int iters = recipe_iterations(ops, count);
+  const std::size_t needed = static_cast<std::size_t>(std::max(iters, 1)) * starts_;
+  if (errs_.size() < needed) errs_ = DeviceBuffer<double>(needed);
+  capacity_ = iters;
+  const Ctrl ctrl{errs_.get(), capacity_, 0.0f, 0.0f, counters_.get()};
+  QPB_CHECK(cudaMemcpyAsync(ctrl_.get(), &ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  QPB_CHECK(cudaMemsetAsync(errs_.get(), 0, needed * sizeof(double), stream_));
+  QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
+  stream_.sync();
+  run_iterations_ = 0;
+  for (std::size_t i = 0; i < count; ++i) {
+    const OpDesc& o = ops[i];
+    switch (o.kind) {
+      case kOpER:
+        iterate(o.n, er_coefficients());
+        break;
+      case kOpHIO:
+        iterate(o.n, hio_coefficients(o.beta));
+        break;
+      case kOpRAAR:
+        iterate(o.n, raar_coefficients(o.beta));
+        break;
+      case kOpShrinkwrap:
+        shrinkwrap(o);
+        break;
+      case kOpDetwinBegin:
+        detwin_begin(o.axis);
+        break;
+      case kOpDetwinEnd:
+        detwin_end();
+        break;
+    }
+  }
+  collect_errors(run_iterations_);
+}
+
+void Solver::iterate(int count, Coefficients c) {
+  if (!wave_valid_) establish_wave();
+  set_coefficients(ctrl_.get(), c.a, c.b, stream_);
+  const int every = options_.sync_every;
+  for (int done = 0; done < count;) {
+    const int len = std::min(count - done, every - iteration_ % every);
+    if (options_.variant == Variant::kBatched) {
+      auto it = graphs_.find(len);
+      if (it == graphs_.end()) {
+        const unsigned long long before = launches();
+        QPB_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int g = 0; g < groups_; ++g) {
+            for (int i = 0; i < len; ++i) enqueue_iteration(g);
+          }
+        } catch (...) {
+          cudaGraph_t broken{};
+          cudaStreamEndCapture(stream_, &broken);
+          if (broken) cudaGraphDestroy(broken);
+          throw;
+        }
+        cudaGraph_t graph{};
+        QPB_CHECK(cudaStreamEndCapture(stream_, &graph));
+        const unsigned long long kernels = launches() - before;
+        count_launches(0ULL - kernels);  // counted again on every replay
+        it = graphs_.emplace(len, std::make_unique<Graph>(graph, kernels)).first;
+      }
+      it->second->launch(stream_);
+    } else {
+      for (int g = 0; g < groups_; ++g) {
+        for (int i = 0; i < len; ++i) enqueue_iteration(g);
+      }
+    }
+    done += len;
+    iteration_ += len;
+    run_iterations_ += len;
+    if (progress_ && iteration_ % every == 0) report();
+  }
+}
+
+int Solver::profile_passes(int iterations, double* ms) {
+  if (iterations < 1) throw InvalidArgument("iterations must be >= 1");
+  if (!wave_valid_) establish_wave();
+  const int outer = runner_.outer();
+  struct PassRef {
+    Mode mode;
+    int axis3;
+  };
+  std::vector<PassRef> passes{{Mode::kMod, outer}};
+  if (runner_.has_mid()) passes.push_back({Mode::kInv, 1});
+  passes.push_back({Mode::kUpd, 2});
+  if (runner_.has_mid()) passes.push_back({Mode::kFwd, 1});
+  const int np = static_cast<int>(passes.size());
+  std::vector<cudaEvent_t> events(static_cast<std::size_t>(2 * np * iterations));
+  for (auto& e : events) QPB_CHECK(cudaEventCreate(&e));
+  for (int it = 0; it < iterations; ++it) {
+    for (int p = 0; p < np; ++p) {
+      QPB_CHECK(cudaEventRecord(events[2 * (it * np + p)], stream_));
+      for (int g = 0; g < groups_; ++g) {
+        runner_.launch(passes[p].mode, passes[p].axis3, base(passes[p].mode, passes[p].axis3, g),
+                       stream_);
+      }
+      QPB_CHECK(cudaEventRecord(events[2 * (it * np + p) + 1], stream_));
+    }
+  }
+  stream_.sync();
+  for (int p = 0; p < np; ++p) {
+    double total = 0.0;
+    for (int it = 0; it < iterations; ++it) {
+      float t = 0.0f;
+      QPB_CHECK(cudaEventElapsedTime(&t, events[2 * (it * np + p)], events[2 * (it * np + p) + 1]));
+      total += t;
+    }
+    ms[p] = total / iterations;
+  }
+  for (auto& e : events) cudaEventDestroy(e);
+  return np;
+}
+
+void Solver::shrinkwrap(const OpDesc& o) {
+  // Blur |x| with exp(-2 (pi sigma f)^2) one axis at a time, reduce the level
+  // in the last pass, threshold (kernels.cpp:77-102).
+  const float half_pi = kTwoPi / 2;
+  const float k = -2.0f * half_pi * half_pi * o.sigma * o.sigma;
+  const int outer = runner_.outer();
+  for (int g = 0; g < groups_; ++g) {
+    QPB_CHECK(cudaMemsetAsync(level_.get(), 0, batch_ * sizeof(LevelAcc), stream_));
+    PassParams first = base(Mode::kBlurMag, outer, g);
+    first.blur_k = k;
+    runner_.launch(Mode::kBlurMag, outer, first, stream_);
+    if (runner_.has_mid()) {
+      PassParams mid = base(Mode::kBlur, 1, g);
+      mid.blur_k = k;
+      runner_.launch(Mode::kBlur, 1, mid, stream_);
+    }
+    PassParams last = base(Mode::kBlur, 2, g);
+    last.blur_k = k;
+    last.level_method = o.method + 1;
+    runner_.launch(Mode::kBlur, 2, last, stream_);
+    shrinkwrap_threshold(w(g), level_.get(), n_, batch_, o.method + 1, o.threshold, support(g),
+                         stream_);
+  }
+  wave_valid_ = false;
+}
+
+void Solver::detwin_begin(int axis) {
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  QPB_CHECK(cudaMemcpyAsync(saved_.get(), support_.get(), total, cudaMemcpyDeviceToDevice, stream_));
+  detwin(support_.get(), moments_.get(), d_, axis + (3 - ndim_), starts_, stream_);
+}
+
+void Solver::detwin_end() {
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  QPB_CHECK(cudaMemcpyAsync(support_.get(), saved_.get(), total, cudaMemcpyDeviceToDevice, stream_));
+}
+
+float Solver::to_error(double num) const {
+  return static_cast<float>(std::sqrt(num / (energy_ + kEps)));
+}
+
+void Solver::collect_errors(int iterations) {
+  host_errs_.resize(static_cast<std::size_t>(std::max(iterations, 1)) * starts_);
+  if (iterations > 0) {
+    QPB_CHECK(cudaMemcpyAsync(host_errs_.data(), errs_.get(),
+                              static_cast<std::size_t>(iterations) * starts_ * sizeof(double),
+                              cudaMemcpyDeviceToHost, stream_));
+  }
+  stream_.sync();
+  for (int t = 0; t < iterations; ++t) {
+    for (int s = 0; s < starts_; ++s) {
+      errors_[s].push_back(to_error(host_errs_[static_cast<std::size_t>(t) * starts_ + s]));
+    }
+  }
+}
+
+void Solver::report() {
+  std::vector<double> row(static_cast<std::size_t>(starts_));
+  QPB_CHECK(cudaMemcpyAsync(row.data(),
+                            errs_.get() + static_cast<std::size_t>(run_iterations_ - 1) * starts_,
+                            row.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  stream_.sync();
+  std::vector<float> latest(row.size());
+  for (std::size_t s = 0; s < row.size(); ++s) latest[s] = to_error(row[s]);
+  progress_(progress_user_, iteration_, latest.data(), starts_);
+}
+
+void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  if (objects) {
+    roll<float2>(x_.get(), w_.get(), d_, starts_, false, stream_);
+    QPB_CHECK(cudaMemcpyAsync(objects, w_.get(), total * sizeof(float2), cudaMemcpyDeviceToHost,
+                              stream_));
+    wave_valid_ = false;
+  }
+  if (supports) {
+    roll<std::uint8_t>(support_.get(), saved_.get(), d_, starts_, false, stream_);
+    QPB_CHECK(cudaMemcpyAsync(supports, saved_.get(), total, cudaMemcpyDeviceToHost, stream_));
+  }
+  stream_.sync();
+  if (errors) {
+    const std::size_t count = error_count();
+    for (int s = 0; s < starts_; ++s) {
+      std::copy(errors_[s].begin(), errors_[s].end(), errors + static_cast<std::size_t>(s) * count);
+    }
+  }
+}
+
+// ------------------------------------------------------------------- operators
+namespace {
+
+struct OperatorContext {
+  Dims3 d;
+  int ndim;
+  PlanCache plans;
+  Stream stream;
+  PassRunner runner;
+  OperatorContext(Dims3 dims, int nd) : d(dims), ndim(nd), runner(dims, nd, plans) {}
+};
+
+ProblemView view_of(int ndim, const long long* shape) {
+  ProblemView v;
+  v.ndim = ndim;
+  if (ndim != 2 && ndim != 3) throw InvalidArgument("shape must be 2D or 3D, got ndim=" + std::to_string(ndim));
+  for (int a = 0; a < ndim; ++a) v.shape[a] = shape[a];
+  return v;
+}
+
+}  // namespace
+
+float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storage) {
+  const Dims3 d = dims_of(problem);
+  const long long n = d.n();
+  OperatorContext ctx(d, problem.ndim);
+  const auto amp = host_roll(problem.amplitude, d, true);
+  std::vector<std::uint8_t> mask(static_cast<std::size_t>(n), 0);
+  if (problem.mask) {
+    mask = host_roll(problem.mask, d, true);
+    for (auto& m : mask) m = m != 0;
+  }
+  const double energy = usable_energy(amp, mask);
+  auto d_amp = upload(signed_amplitude(amp, mask, storage), ctx.stream);
+  auto d_x = upload(host_roll(obj, d, true), ctx.stream);
+  DeviceBuffer<float2> d_w(static_cast<std::size_t>(n));
+  DeviceBuffer<double> errs(1);
+  DeviceBuffer<int> counter(1);
+  DeviceBuffer<Ctrl> ctrl(1);
+  QPB_CHECK(cudaMemsetAsync(errs.get(), 0, sizeof(double), ctx.stream));
+  QPB_CHECK(cudaMemsetAsync(counter.get(), 0, sizeof(int), ctx.stream));
+  const Ctrl c{errs.get(), 1, 0.0f, 0.0f, counter.get()};
+  QPB_CHECK(cudaMemcpyAsync(ctrl.get(), &c, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx.stream));
+  auto params = [&](Mode m, int axis3) {
+    PassParams p = ctx.runner.params(m, axis3, 1);
+    p.w = d_w.get();
+    p.x = d_x.get();
+    p.amp = d_amp.get();
+    p.ctrl = ctrl.get();
+    p.starts_total = 1;
+    p.amp_storage = storage;
+    return p;
+  };
+  const int outer = ctx.runner.outer();
+  ctx.runner.launch(Mode::kFwdFromX, 2, params(Mode::kFwdFromX, 2), ctx.stream);
+  if (ctx.runner.has_mid()) ctx.runner.launch(Mode::kFwd, 1, params(Mode::kFwd, 1), ctx.stream);
+  ctx.runner.launch(Mode::kMod, outer, params(Mode::kMod, outer), ctx.stream);
+  if (ctx.runner.has_mid()) ctx.runner.launch(Mode::kInv, 1, params(Mode::kInv, 1), ctx.stream);
+  ctx.runner.launch(Mode::kInv, 2, params(Mode::kInv, 2), ctx.stream);
+  std::vector<float2> host(static_cast<std::size_t>(n));
+  double num = 0.0;
+  QPB_CHECK(cudaMemcpyAsync(host.data(), d_w.get(), host.size() * sizeof(float2),
+                            cudaMemcpyDeviceToHost, ctx.stream));
+  QPB_CHECK(cudaMemcpyAsync(&num, errs.get(), sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.stream.sync();
+  const auto centred = host_roll(host.data(), d, false);
+  std::copy(centred.begin(), centred.end(), obj);
+  return static_cast<float>(std::sqrt(num / (energy + kEps)));
+}
+
+void support_project_host(const std::uint8_t* support, float2* obj, long long count) {
+  Stream s;
+  DeviceBuffer<float2> x(static_cast<std::size_t>(count));
+  DeviceBuffer<std::uint8_t> sup(static_cast<std::size_t>(count));
+  QPB_CHECK(cudaMemcpyAsync(x.get(), obj, count * sizeof(float2), cudaMemcpyHostToDevice, s));
+  QPB_CHECK(cudaMemcpyAsync(sup.get(), support, count, cudaMemcpyHostToDevice, s));
+  support_project(x.get(), sup.get(), count, 1, s);
+  QPB_CHECK(cudaMemcpyAsync(obj, x.get(), count * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  s.sync();
+}
+
+void gaussian_blur(const float* image, int ndim, const long long* shape, float sigma, float* out) {
+  const Dims3 d = dims_of(view_of(ndim, shape));
+  if (!(sigma >= 0.0f)) throw InvalidArgument("sigma must be >= 0");
+  const long long n = d.n();
+  OperatorContext ctx(d, ndim);
+  // A circular blur commutes with the fftshift roll (operators.cpp:33-39).
+  std::vector<float2> host(static_cast<std::size_t>(n));
+  for (long long i = 0; i < n; ++i) host[i] = {image[i], 0.0f};
+  auto w = upload(host, ctx.stream);
+  const float half_pi = kTwoPi / 2;
+  const float k = -2.0f * half_pi * half_pi * sigma * sigma;
+  for (int axis3 = ctx.runner.outer(); axis3 < 3; ++axis3) {
+    PassParams p = ctx.runner.params(Mode::kBlur, axis3, 1);
+    p.w = w.get();
+    p.blur_k = k;
+    ctx.runner.launch(Mode::kBlur, axis3, p, ctx.stream);
+  }
+  QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
+                            cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.stream.sync();
+  for (long long i = 0; i < n; ++i) out[i] = host[i].x;
+}
+
+void autocorrelation_support(const float* intensity, int ndim, const long long* shape,
+                             float threshold, std::uint8_t* out) {
+  const Dims3 d = dims_of(view_of(ndim, shape));
+  const long long n = d.n();
+  OperatorContext ctx(d, ndim);
+  const auto ordered = host_roll(intensity, d, true);
+  std::vector<float2> host(static_cast<std::size_t>(n));
+  for (long long i = 0; i < n; ++i) host[i] = {ordered[i], 0.0f};
+  auto w = upload(host, ctx.stream);
+  for (int axis3 = ctx.runner.outer(); axis3 < 3; ++axis3) {
+    PassParams p = ctx.runner.params(Mode::kInv, axis3, 1);
+    p.w = w.get();
+    ctx.runner.launch(Mode::kInv, axis3, p, ctx.stream);
+  }
+  QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
+                            cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.stream.sync();
+  // Unitary scale, |.|, centre-origin, threshold against the maximum.
+  const float s = 1.0f / std::sqrt(static_cast<float>(n));
+  std::vector<float> ac(static_cast<std::size_t>(n));
+  for (long long i = 0; i < n; ++i) {
+    const float re = host[i].x * s, im = host[i].y * s;
+    ac[i] = std::sqrt(re * re + im * im);
+  }
+  const auto centred = host_roll(ac.data(), d, false);
+  const float level = threshold * *std::max_element(centred.begin(), centred.end());
+  for (long long i = 0; i < n; ++i) out[i] = centred[i] > level;
+}
+
+void half_support(const std::uint8_t* support, int ndim, const long long* shape, int axis,
+                  std::uint8_t* out) {
+  const Dims3 d = dims_of(view_of(ndim, shape));
+  if (axis < 0 || axis >= ndim) throw InvalidArgument("detwin axis out of range");
+  const long long n = d.n();
+  Stream s;
+  auto ordered = host_roll(support, d, true);
+  for (auto& v : ordered) v = v != 0;
+  auto dev = upload(ordered, s);
+  DeviceBuffer<unsigned long long> moments(2);
+  detwin(dev.get(), moments.get(), d, axis + (3 - ndim), 1, s);
+  QPB_CHECK(cudaMemcpyAsync(ordered.data(), dev.get(), static_cast<std::size_t>(n),
+                            cudaMemcpyDeviceToHost, s));
+  s.sync();
+  const auto centred = host_roll(ordered.data(), d, false);
+  std::copy(centred.begin(), centred.end(), out);
+}
+
+}  // namespace qpb

@@ -1,0 +1,252 @@
+// The B200 reconstruction solver: every start's iterate resident in HBM in FFT
+// order, iterations as fused line passes, batched starts captured in CUDA
+// graphs. It implements the contract of QoraPhaseCU's qpcu::Solver
+// (include/qoraphasecu/solver.hpp:67-74): construction draws the starts, run()
+// continues from the current state and appends one error per iteration,
+// results() returns centre-origin objects, supports and error histories.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "common.cuh"
+#include "fft_plan.hpp"
+#include "line_pass.cuh"
+
+namespace qpb {
+
+// Owning device allocation.
+template <class T>
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(std::size_t count) : count_(count) {
+    if (count) QPB_CHECK(cudaMalloc(reinterpret_cast<void**>(&ptr_), count * sizeof(T)));
+  }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), count_(o.count_) {
+    o.ptr_ = nullptr;
+    o.count_ = 0;
+  }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    std::swap(ptr_, o.ptr_);
+    std::swap(count_, o.count_);
+    return *this;
+  }
+  ~DeviceBuffer() {
+    if (ptr_) cudaFree(ptr_);
+  }
+  T* get() const { return ptr_; }
+  std::size_t size() const { return count_; }
+
+ private:
+  T* ptr_ = nullptr;
+  std::size_t count_ = 0;
+};
+
+// A stream the object creates (and destroys), or one the caller lends.
+class Stream {
+ public:
+  Stream() { QPB_CHECK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking)); }
+  explicit Stream(cudaStream_t borrowed) : s_(borrowed), owned_(borrowed == nullptr) {
+    if (owned_) QPB_CHECK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+  }
+  Stream(const Stream&) = delete;
+  Stream& operator=(const Stream&) = delete;
+  ~Stream() {
+    if (owned_) cudaStreamDestroy(s_);
+  }
+  operator cudaStream_t() const { return s_; }
+  void sync() const { QPB_CHECK(cudaStreamSynchronize(s_)); }
+
+ private:
+  cudaStream_t s_{};
+  bool owned_ = true;
+};
+
+
+
+class Graph {
+ public:
+  Graph(cudaGraph_t g, unsigned long long kernels) : kernels_(kernels) {
+    QPB_CHECK(cudaGraphInstantiate(&exec_, g, 0));
+    cudaGraphDestroy(g);
+  }
+  Graph(const Graph&) = delete;
+  Graph& operator=(const Graph&) = delete;
+  ~Graph() { cudaGraphExecDestroy(exec_); }
+  void launch(cudaStream_t s) const {
+    QPB_CHECK(cudaGraphLaunch(exec_, s));
+    count_launches(kernels_);
+  }
+
+ private:
+  cudaGraphExec_t exec_{};
+  unsigned long long kernels_;
+};
+
+// Centre-origin problem arrays (QoraPhaseCU's qpcu::Problem, problem.hpp:26-31).
+struct ProblemView {
+  int ndim = 0;
+  long long shape[3] = {0, 0, 0};
+  const float* amplitude = nullptr;     // sqrt(clip(I, 0)), numel
+  const std::uint8_t* mask = nullptr;   // 1 = unusable; null = none
+  const std::uint8_t* support = nullptr;  // 1 = inside
+};
+
+enum class Variant : int {
+  kBatched = 0,  // `batch` starts per launch, iterations replayed from CUDA graphs
+  kPlain = 1,    // one start per launch, launched directly: the in-repo baseline
+};
+
+struct SolverOptions {
+  int starts = 1;
+  int batch = 0;  // starts per launch; 0 = all (kBatched only)
+  std::uint64_t seed = 0;
+  const float2* start = nullptr;  // starts * numel centre-origin objects, or null
+  int sync_every = 10;
+  Variant variant = Variant::kBatched;
+  AmpStorage amp_storage = AmpStorage::kF32;
+  int device = -1;                  // CUDA ordinal; -1 = the current device
+  cudaStream_t stream = nullptr;    // work stream lent by the caller; null = own stream
+};
+
+// One recipe operation, the POD form of qpcu::Op (recipe.hpp:44).
+enum OpKind : int { kOpER = 0, kOpHIO = 1, kOpRAAR = 2, kOpShrinkwrap = 3, kOpDetwinBegin = 4,
+                    kOpDetwinEnd = 5 };
+struct OpDesc {
+  int kind;
+  int n;
+  float beta;
+  float threshold;
+  float sigma;
+  int method;  // 0 max, 1 rms
+  int axis;
+};
+
+using ProgressFn = void (*)(void* user, int iteration, const float* errors, int count);
+
+// Checks shape rank and extents; returns Dims3 (2D -> {1, ny, nx}).
+Dims3 dims_of(const ProblemView& p);
+void validate_recipe(const OpDesc* ops, std::size_t count);
+int recipe_iterations(const OpDesc* ops, std::size_t count);
+
+// Enqueues the line passes of one array stack on a stream.
+class PassRunner {
+ public:
+  PassRunner(Dims3 d, int ndim, PlanCache& plans);
+
+  PassParams params(Mode mode, int axis3, int batch) const;
+  void launch(Mode mode, int axis3, PassParams p, cudaStream_t s) const;
+  int outer() const { return ndim_ == 2 ? 1 : 0; }
+  bool has_mid() const { return ndim_ == 3; }
+  Dims3 dims() const { return d_; }
+
+ private:
+  Dims3 d_;
+  int ndim_;
+  const LinePlan* plans_[3];
+};
+
+class Solver {
+ public:
+  Solver(const ProblemView& problem, const SolverOptions& options);
+  ~Solver();
+  Solver(const Solver&) = delete;
+  Solver& operator=(const Solver&) = delete;
+
+  void run(const OpDesc* ops, std::size_t count);
+  std::size_t error_count() const { return errors_.empty() ? 0 : errors_[0].size(); }
+  int starts() const { return starts_; }
+  long long numel() const { return n_; }
+  int device() const { return select_.device; }
+  // objects: starts * numel complex64; supports: starts * numel; errors: starts * error_count().
+  void results(float2* objects, std::uint8_t* supports, float* errors);
+  void set_progress(ProgressFn fn, void* user) {
+    progress_ = fn;
+    progress_user_ = user;
+  }
+  // Runs `iterations` iterations with every pass launched directly between
+  // CUDA events; ms[p] receives the mean duration of pass p of an iteration.
+  // Returns the number of passes per iteration (at most 8). Advances the state.
+  int profile_passes(int iterations, double* ms);
+
+ private:
+  float2* x(int g) const { return x_.get() + static_cast<std::size_t>(g) * batch_ * n_; }
+  float2* w(int g) const { return w_.get() + static_cast<std::size_t>(g) * batch_ * n_; }
+  std::uint8_t* support(int g) const {
+    return support_.get() + static_cast<std::size_t>(g) * batch_ * n_;
+  }
+  PassParams base(Mode mode, int axis3, int g) const;
+
+  void enqueue_iteration(int g);
+  void enqueue_establish(int g);
+  void establish_wave();
+  void iterate(int count, Coefficients c);
+  void shrinkwrap(const OpDesc& o);
+  void detwin_begin(int axis);
+  void detwin_end();
+  void collect_errors(int iterations);
+  void report();
+  float to_error(double num) const;
+
+  Dims3 d_;
+  int ndim_;
+  long long n_;
+  int starts_;
+  int batch_;
+  int groups_;
+  SolverOptions options_;
+  // Selects the device before any allocation; every later call re-selects it.
+  struct DeviceSelect {
+    int device = 0;
+    explicit DeviceSelect(int requested) {
+      if (requested >= 0) QPB_CHECK(cudaSetDevice(requested));
+      QPB_CHECK(cudaGetDevice(&device));
+    }
+  } select_;
+  PlanCache plans_;
+  Stream stream_;
+  PassRunner runner_;
+  double energy_ = 0.0;
+  DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
+  DeviceBuffer<float2> x_;
+  DeviceBuffer<float2> w_;
+  DeviceBuffer<std::uint8_t> support_;
+  DeviceBuffer<std::uint8_t> saved_;
+  DeviceBuffer<LevelAcc> level_;
+  DeviceBuffer<unsigned long long> moments_;
+  DeviceBuffer<Ctrl> ctrl_;
+  DeviceBuffer<int> counters_;
+  DeviceBuffer<double> errs_;
+  int capacity_ = 0;
+  bool wave_valid_ = false;
+  std::map<int, std::unique_ptr<Graph>> graphs_;
+  std::vector<std::vector<float>> errors_;
+  std::vector<double> host_errs_;
+  int iteration_ = 0;
+  int run_iterations_ = 0;
+  ProgressFn progress_ = nullptr;
+  void* progress_user_ = nullptr;
+};
+
+// ---- single operators on centre-origin arrays (operators.hpp:13-33)
+// Replaces obj (numel complex64, centre-origin) by P_M obj; returns the Fourier
+// error of the input.
+float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storage);
+void support_project_host(const std::uint8_t* support, float2* obj, long long count);
+void gaussian_blur(const float* image, int ndim, const long long* shape, float sigma, float* out);
+// Loose support: |IFFT(intensity)| > threshold * max, centre-origin (problem.cpp:72-88).
+void autocorrelation_support(const float* intensity, int ndim, const long long* shape,
+                             float threshold, std::uint8_t* out);
+// half_support on the device (problem.cpp:101-127), centre-origin in and out.
+void half_support(const std::uint8_t* support, int ndim, const long long* shape, int axis,
+                  std::uint8_t* out);
+
+}  // namespace qpb
