@@ -260,7 +260,7 @@ def main(argv=None):
     barrier()
 
     step_ms = []
-    launches0 = qpc.kernel_launches()
+    launches0 = qpc.api.kernel_launches()
     t_wall = time.perf_counter()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
@@ -274,7 +274,7 @@ def main(argv=None):
             step_ms.append(e0.elapsed_time(e1))
         barrier()
     wall_s = time.perf_counter() - t_wall
-    launches = qpc.kernel_launches() - launches0
+    launches = qpc.api.kernel_launches() - launches0
     total_ms = max_over_ranks(sum(step_ms))
     value = world * STARTS * iters * args.steps / (total_ms / 1e3)
 

@@ -16,6 +16,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define QPB_API __attribute__((visibility("default")))
+#else
+#define QPB_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -88,62 +94,62 @@ typedef struct qpb_solver qpb_solver;
 typedef void (*qpb_progress_fn)(void* user, int iteration, const float* errors, int count);
 
 /* Message of the last failed call on this thread ("" if none). */
-const char* qpb_last_error(void);
+QPB_API const char* qpb_last_error(void);
 
 /* 1 when a CUDA device is present (qpcu::cuda_available, solver.hpp:85). */
-int qpb_cuda_available(void);
+QPB_API int qpb_cuda_available(void);
 
 /* Selects the device that calls without a solver (make_problem, the single
  * operators) use on the calling thread. No counterpart in the reference, which
  * always uses the current device (src/cuda/kernels.cu:15-24). */
-qpb_status qpb_set_device(int device);
+QPB_API qpb_status qpb_set_device(int device);
 
 /* Replaces qpcu::cuda_device_info (solver.hpp:87-98). name_out holds name_len bytes. */
-qpb_status qpb_device_info(char* name_out, size_t name_len, int* sm_major, int* sm_minor,
+QPB_API qpb_status qpb_device_info(char* name_out, size_t name_len, int* sm_major, int* sm_minor,
                            size_t* memory_bytes, size_t* l2_bytes, double* peak_bandwidth_gbs);
 
 /* qpcu::make_problem (problem.hpp:35-37, problem.cpp:40-70): validates the
  * inputs, amplitude = sqrt(max(I, 0)); a NULL support is replaced by the
  * autocorrelation support at `support_threshold`. Outputs are numel each. */
-qpb_status qpb_make_problem(const float* intensity, int ndim, const int64_t* shape,
+QPB_API qpb_status qpb_make_problem(const float* intensity, int ndim, const int64_t* shape,
                             const uint8_t* support, const uint8_t* mask, float support_threshold,
                             float* amplitude_out, uint8_t* mask_out, uint8_t* support_out);
 
 /* qpcu::autocorrelation_support (problem.hpp:42-43, problem.cpp:72-88). */
-qpb_status qpb_autocorrelation_support(const float* intensity, int ndim, const int64_t* shape,
+QPB_API qpb_status qpb_autocorrelation_support(const float* intensity, int ndim, const int64_t* shape,
                                        float threshold, uint8_t* out);
 
 /* qpcu::half_support (problem.hpp:51-52, problem.cpp:101-127), on the device. */
-qpb_status qpb_half_support(const uint8_t* support, int ndim, const int64_t* shape, int axis,
+QPB_API qpb_status qpb_half_support(const uint8_t* support, int ndim, const int64_t* shape, int axis,
                             uint8_t* out);
 
 /* qpcu::make_solver for the new backend (solver.cpp:61-86 ->
  * detail::make_cuda_solver, backends.hpp:9-10): uploads the problem and draws
  * the starts. */
-qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out);
+QPB_API qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out);
 
 /* qpcu::Solver::run (solver.hpp:72): validates and runs the recipe, continuing
  * from the current state; appends one error per iteration to every start. */
-qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);
+QPB_API qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);
 
 /* Progress callback (Options::progress, solver.hpp:52-54); NULL disables it. */
-qpb_status qpb_set_progress(qpb_solver* solver, qpb_progress_fn fn, void* user);
+QPB_API qpb_status qpb_set_progress(qpb_solver* solver, qpb_progress_fn fn, void* user);
 
 /* Iterations run so far (the length of every start's error history). */
-qpb_status qpb_error_count(const qpb_solver* solver, size_t* count);
-qpb_status qpb_starts(const qpb_solver* solver, int* starts);
+QPB_API qpb_status qpb_error_count(const qpb_solver* solver, size_t* count);
+QPB_API qpb_status qpb_starts(const qpb_solver* solver, int* starts);
 
 /* qpcu::Solver::results (solver.hpp:73) into caller buffers: objects
  * starts * numel complex64, supports starts * numel, errors starts * error_count.
  * Any output may be NULL. */
-qpb_status qpb_results(qpb_solver* solver, float* objects, uint8_t* supports, float* errors);
+QPB_API qpb_status qpb_results(qpb_solver* solver, float* objects, uint8_t* supports, float* errors);
 
-void qpb_destroy(qpb_solver* solver);
+QPB_API void qpb_destroy(qpb_solver* solver);
 
 /* Kernels this library has launched in this process; a replayed CUDA graph
  * counts each kernel node. No counterpart in the reference: it backs the
  * launch count that bench.py reports. */
-uint64_t qpb_kernel_launches(void);
+QPB_API uint64_t qpb_kernel_launches(void);
 
 /* Runs `iterations` more iterations with every line pass launched directly
  * between CUDA events on the solver's stream; ms_out[p] receives the mean
@@ -151,13 +157,13 @@ uint64_t qpb_kernel_launches(void);
  * the y-axis inverse and forward passes) and *n_passes their count (<= 8).
  * Advances the iterate. No counterpart in the reference: it feeds the
  * per-kernel roofline that bench.py reports. */
-qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
+QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
 
 /* Single operators on centre-origin arrays (qpcu::cuda::, operators.hpp:25-33). */
-qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
+QPB_API qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
                                float* error_out);
-qpb_status qpb_support_project(const uint8_t* support, float* obj, size_t count);
-qpb_status qpb_gaussian_blur(const float* image, int ndim, const int64_t* shape, float sigma,
+QPB_API qpb_status qpb_support_project(const uint8_t* support, float* obj, size_t count);
+QPB_API qpb_status qpb_gaussian_blur(const float* image, int ndim, const int64_t* shape, float sigma,
                              float* out);
 
 #ifdef __cplusplus

@@ -20,8 +20,10 @@ from .api import (
     best_index,
     cuda_available,
     half_support,
+    kernel_launches,
     make_problem,
     reconstruct,
+    set_device,
 )
 from .operators import gaussian_blur, modulus_project, support_project
 from .recipe import ER, HIO, RAAR, Recipe, Shrinkwrap, default_recipe, detwin, repeat

@@ -29,6 +29,8 @@ NVCC_FLAGS = [
     "-std=c++20",
     "-Xcompiler", "-fPIC",
     "-Xcompiler", "-Wall",
+    "-Xcompiler", "-g",
+    "-Xcompiler", "-fvisibility=hidden",
     "--expt-relaxed-constexpr",
     "-I", str(ROOT / "include"),
 ]

@@ -124,6 +124,8 @@ __global__ void set_coefficients_kernel(Ctrl* ctrl, float a, float b) {
   ctrl->b = b;
 }
 
+__global__ void set_ctrl_kernel(Ctrl* ctrl, Ctrl value) { *ctrl = value; }
+
 __global__ void scale_complex_kernel(float2* x, long long count, float scale) {
   QPB_FOR(i, count) { x[i] = cscale(x[i], scale); }
 }
@@ -183,6 +185,12 @@ template void roll<std::uint8_t>(const std::uint8_t*, std::uint8_t*, Dims3, int,
 
 void set_coefficients(Ctrl* ctrl, float a, float b, cudaStream_t stream) {
   set_coefficients_kernel<<<1, 1, 0, stream>>>(ctrl, a, b);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+void set_ctrl(Ctrl* ctrl, const Ctrl& value, cudaStream_t stream) {
+  set_ctrl_kernel<<<1, 1, 0, stream>>>(ctrl, value);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }

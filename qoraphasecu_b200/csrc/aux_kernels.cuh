@@ -40,6 +40,10 @@ void roll(const T* in, T* out, Dims3 d, int batch, bool to_fft_order, cudaStream
 // Writes the control block fields of a stage.
 void set_coefficients(Ctrl* ctrl, float a, float b, cudaStream_t stream);
 
+// Writes a whole control block on `stream` (kernel arguments, so no host
+// buffer has to outlive the call).
+void set_ctrl(Ctrl* ctrl, const Ctrl& value, cudaStream_t stream);
+
 // x[b][i] = x[b][i] / scale (complex), used for results of scaled storage.
 void scale_complex(float2* x, long long count, float scale, cudaStream_t stream);
 

@@ -71,6 +71,11 @@ qpb::AmpStorage storage_of(int s) {
   return static_cast<qpb::AmpStorage>(s);
 }
 
+// The runtime's current device is per host thread: make the solver's current.
+void use_solver_device(const qpb_solver* solver) {
+  QPB_CHECK(cudaSetDevice(solver->impl.device()));
+}
+
 }  // namespace
 
 extern "C" {
@@ -191,22 +196,30 @@ qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qp
     o.device = options->device;
     o.stream = static_cast<cudaStream_t>(options->stream);
     if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
+    qpb::trace("qpb_create: starts=%d batch=%d variant=%d shape=%lld,%lld,%lld", o.starts, o.batch,
+               options->variant, v.shape[0], v.shape[1], v.shape[2]);
     *out = new qpb_solver(v, o);
+    qpb::trace("qpb_create: solver %p ready", static_cast<void*>(*out));
   });
 }
-
-namespace {
-// The runtime's current device is per host thread: select the solver's.
-void select(const qpb_solver* solver) { QPB_CHECK(cudaSetDevice(solver->impl.device())); }
-}  // namespace
 
 qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops) {
   return guarded([&] {
     require(solver != nullptr, "solver is NULL");
     require(ops != nullptr || n_ops == 0, "ops is NULL");
     static_assert(sizeof(qpb_op) == sizeof(qpb::OpDesc));
+    if (qpb::tracing()) {
+      qpb::trace("qpb_run solver=%p ops=%p n_ops=%zu", static_cast<void*>(solver),
+                 static_cast<const void*>(ops), n_ops);
+      for (size_t i = 0; i < n_ops; ++i) {
+        qpb::trace("  op[%zu] kind=%d n=%d beta=%g thr=%g sigma=%g method=%d axis=%d", i,
+                   ops[i].kind, ops[i].n, ops[i].beta, ops[i].threshold, ops[i].sigma,
+                   ops[i].method, ops[i].axis);
+      }
+    }
     qpb::validate_recipe(reinterpret_cast<const qpb::OpDesc*>(ops), n_ops);
-    select(solver);
+    qpb::trace("qpb_run: recipe valid, selecting device %d", solver->impl.device());
+    use_solver_device(solver);
     solver->impl.run(reinterpret_cast<const qpb::OpDesc*>(ops), n_ops);
   });
 }
@@ -216,7 +229,7 @@ uint64_t qpb_kernel_launches(void) { return qpb::launches(); }
 qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes) {
   return guarded([&] {
     require(solver && ms_out && n_passes, "NULL argument");
-    select(solver);
+    use_solver_device(solver);
     *n_passes = solver->impl.profile_passes(iterations, ms_out);
   });
 }
@@ -245,7 +258,7 @@ qpb_status qpb_starts(const qpb_solver* solver, int* starts) {
 qpb_status qpb_results(qpb_solver* solver, float* objects, uint8_t* supports, float* errors) {
   return guarded([&] {
     require(solver != nullptr, "solver is NULL");
-    select(solver);
+    use_solver_device(solver);
     solver->impl.results(reinterpret_cast<float2*>(objects), supports, errors);
   });
 }

@@ -83,4 +83,8 @@ inline void cuda_check(cudaError_t status, const char* what) {
 void count_launches(unsigned long long n);
 unsigned long long launches();
 
+// Host-side trace to stderr when the environment sets QPB_TRACE=1.
+bool tracing();
+void trace(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+
 }  // namespace qpb

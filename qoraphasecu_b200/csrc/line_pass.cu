@@ -10,6 +10,8 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 
 #include "butterfly.cuh"
@@ -296,15 +298,23 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(const PassParams p)
   }
 }
 
+// Largest dynamic shared memory a line pass asks for (choose_lpc keeps the two
+// buffers at or below this).
+constexpr int kMaxPassSmem = 2 * 16 * 512 * static_cast<int>(sizeof(float2));
+
+template <class Kernel>
+void allow_smem(Kernel kernel) {
+  QPB_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
+}
+
 template <Mode M>
 void launch_mode(const PassParams& p, cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(p.lines / p.lpc));
   const std::size_t smem = 2u * static_cast<std::size_t>(p.lpc) * p.L * sizeof(float2);
+  if (smem > static_cast<std::size_t>(kMaxPassSmem)) {
+    throw std::logic_error("line pass: shared memory request above the configured maximum");
+  }
   auto launch = [&](auto kernel) {
-    if (smem > 48 * 1024) {
-      QPB_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-    }
     kernel<<<grid, kThreads, smem, stream>>>(p);
     QPB_CHECK(cudaGetLastError());
     count_launches(1);
@@ -327,6 +337,25 @@ void launch_mode(const PassParams& p, cudaStream_t stream) {
 }
 
 }  // namespace
+
+void configure_line_passes() {
+  // Once per device, outside any stream capture.
+  static std::mutex mutex;
+  static std::set<int> done;
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  if (!done.insert(device).second) return;
+  allow_smem(line_pass_kernel<Mode::kFwd, float>);
+  allow_smem(line_pass_kernel<Mode::kFwdFromX, float>);
+  allow_smem(line_pass_kernel<Mode::kInv, float>);
+  allow_smem(line_pass_kernel<Mode::kMod, float>);
+  allow_smem(line_pass_kernel<Mode::kMod, __half>);
+  allow_smem(line_pass_kernel<Mode::kMod, __nv_bfloat16>);
+  allow_smem(line_pass_kernel<Mode::kUpd, float>);
+  allow_smem(line_pass_kernel<Mode::kBlur, float>);
+  allow_smem(line_pass_kernel<Mode::kBlurMag, float>);
+}
 
 int choose_lpc(int L, int S, int lines_per_start) {
   // About 2048 elements per CTA (32 KiB for the two buffers), at least one line,

@@ -80,6 +80,10 @@ struct PassParams {
 // Launches one generic line pass on `stream`.
 void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream);
 
+// Raises the shared-memory limit of every line-pass kernel on the current
+// device; called once per device before the first launch (never during capture).
+void configure_line_passes();
+
 // Lines per CTA for a line of length L with `lines_per_start` lines per start.
 int choose_lpc(int L, int S, int lines_per_start);
 

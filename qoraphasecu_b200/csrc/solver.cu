@@ -1,9 +1,16 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <execinfo.h>
+#include <unistd.h>
+
+#include <csignal>
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -17,6 +24,46 @@ std::atomic<unsigned long long> g_launches{0};
 
 void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+void crash_handler(int sig) {
+  void* frames[64];
+  const int n = backtrace(frames, 64);
+  const char msg[] = "[qpb] fatal signal, native backtrace:\n";
+  (void)!write(2, msg, sizeof(msg) - 1);
+  backtrace_symbols_fd(frames, n, 2);
+  signal(sig, SIG_DFL);
+  raise(sig);
+}
+}  // namespace
+
+// QPB_TRACE=1 logs host-side steps; any non-zero value (e.g. "backtrace") also
+// prints a native backtrace on SIGSEGV.
+bool tracing() {
+  static const bool on = [] {
+    const char* v = std::getenv("QPB_TRACE");
+    const bool enabled = v && *v && std::strcmp(v, "0") != 0;
+    if (enabled) signal(SIGSEGV, crash_handler);
+    return enabled && std::strcmp(v, "1") == 0;
+  }();
+  return on;
+}
+
+namespace {
+// Installs the crash handler at load time when QPB_TRACE asks for it.
+const bool g_trace_init = (tracing(), true);
+}  // namespace
+
+void trace(const char* fmt, ...) {
+  if (!tracing()) return;
+  std::va_list args;
+  va_start(args, fmt);
+  std::fputs("[qpb] ", stderr);
+  std::vfprintf(stderr, fmt, args);
+  std::fputc('\n', stderr);
+  std::fflush(stderr);
+  va_end(args);
+}
 
 namespace {
 
@@ -153,6 +200,7 @@ int recipe_iterations(const OpDesc* ops, std::size_t count) {
 
 // ------------------------------------------------------------------ PassRunner
 PassRunner::PassRunner(Dims3 d, int ndim, PlanCache& plans) : d_(d), ndim_(ndim) {
+  configure_line_passes();
   for (int a = 0; a < 3; ++a) {
     plans_[a] = (ndim == 2 && a == 0) ? nullptr : &plans.get(axis_len(d, a));
   }
@@ -227,7 +275,7 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
   const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
-  QPB_CHECK(cudaMemcpyAsync(ctrl_.get(), &ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  set_ctrl(ctrl_.get(), ctrl, stream_);
   QPB_CHECK(cudaMemcpyAsync(support_.get(), sup.data(), sup.size(), cudaMemcpyHostToDevice, stream_));
   for (int s = 1; s < starts_; ++s) {
     QPB_CHECK(cudaMemcpyAsync(support_.get() + static_cast<std::size_t>(s) * n_, support_.get(),
@@ -316,16 +364,20 @@ void Solver::run(const OpDesc* ops, std::size_t count) {
   }
   const int iters = recipe_iterations(ops, count);
   const std::size_t needed = static_cast<std::size_t>(std::max(iters, 1)) * starts_;
+  trace("run: %d iterations, errs %zu -> %zu", iters, errs_.size(), needed);
   if (errs_.size() < needed) errs_ = DeviceBuffer<double>(needed);
   capacity_ = iters;
   const Ctrl ctrl{errs_.get(), capacity_, 0.0f, 0.0f, counters_.get()};
-  QPB_CHECK(cudaMemcpyAsync(ctrl_.get(), &ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream_));
+  set_ctrl(ctrl_.get(), ctrl, stream_);
   QPB_CHECK(cudaMemsetAsync(errs_.get(), 0, needed * sizeof(double), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
+  trace("run: control block written");
   stream_.sync();
+  trace("run: synchronized");
   run_iterations_ = 0;
   for (std::size_t i = 0; i < count; ++i) {
     const OpDesc& o = ops[i];
+    trace("run op %zu/%zu kind=%d n=%d (iteration %d)", i, count, o.kind, o.n, iteration_);
     switch (o.kind) {
       case kOpER:
         iterate(o.n, er_coefficients());
@@ -358,6 +410,7 @@ void Solver::iterate(int count, Coefficients c) {
     const int len = std::min(count - done, every - iteration_ % every);
     if (options_.variant == Variant::kBatched) {
       auto it = graphs_.find(len);
+      trace("iterate chunk len=%d graph=%s", len, it == graphs_.end() ? "capture" : "cached");
       if (it == graphs_.end()) {
         const unsigned long long before = launches();
         QPB_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -471,6 +524,7 @@ float Solver::to_error(double num) const {
 }
 
 void Solver::collect_errors(int iterations) {
+  trace("collect_errors iterations=%d starts=%d", iterations, starts_);
   host_errs_.resize(static_cast<std::size_t>(std::max(iterations, 1)) * starts_);
   if (iterations > 0) {
     QPB_CHECK(cudaMemcpyAsync(host_errs_.data(), errs_.get(),
@@ -559,7 +613,7 @@ float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storag
   QPB_CHECK(cudaMemsetAsync(errs.get(), 0, sizeof(double), ctx.stream));
   QPB_CHECK(cudaMemsetAsync(counter.get(), 0, sizeof(int), ctx.stream));
   const Ctrl c{errs.get(), 1, 0.0f, 0.0f, counter.get()};
-  QPB_CHECK(cudaMemcpyAsync(ctrl.get(), &c, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx.stream));
+  set_ctrl(ctrl.get(), c, ctx.stream);
   auto params = [&](Mode m, int axis3) {
     PassParams p = ctx.runner.params(m, axis3, 1);
     p.w = d_w.get();
