@@ -159,6 +159,28 @@ QPB_API uint64_t qpb_kernel_launches(void);
  * per-kernel roofline that bench.py reports. */
 QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
 
+/* The modulus projection of qpb_modulus_project for callers that must not
+ * allocate device memory (no counterpart in the reference): applications that
+ * reserve their whole GPU memory up front and may not grow it, and threads that
+ * cannot afford cudaMalloc's implicit device synchronisation. It allocates
+ * nothing; its scratch lives in one fixed __device__ array of the library.
+ *   Every pointer except `shape` is device memory, arrays in FFT order (numpy
+ * ifftshift of the centre-origin arrays): amplitude (numel float), mask (numel
+ * uint8, NULL = all usable), x (numel complex64), out (numel complex64, may be
+ * x), error_out (1 float: the Fourier error of x). Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) and the call
+ * returns without waiting for it.
+ *   Limits: at most 65536 elements and 4096 along any axis; larger shapes
+ * return QPB_INVALID_ARGUMENT. The first call on a device looks up the array's
+ * device address and configures kernels; make that first call before any
+ * stream capture. All calls on a device share the array, which keeps the last
+ * call's contents (each call clears what must start at zero): calls that
+ * overlap on the GPU, e.g. on two streams, race on it. */
+QPB_API qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape,
+                                               const float* amplitude, const uint8_t* mask,
+                                               const float* x, float* out, float* error_out,
+                                               void* stream);
+
 /* Single operators on centre-origin arrays (qpcu::cuda::, operators.hpp:25-33). */
 QPB_API qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
                                float* error_out);

@@ -51,6 +51,7 @@ EXPORTS = (
     "qpb_destroy",
     "qpb_kernel_launches",
     "qpb_profile_passes",
+    "qpb_modulus_project_noalloc",
     "qpb_modulus_project",
     "qpb_support_project",
     "qpb_gaussian_blur",
@@ -138,6 +139,8 @@ def load():
         lib.qpb_kernel_launches.restype = c_uint64
         lib.qpb_profile_passes.argtypes = [c_void_p, c_int, POINTER(c_double), POINTER(c_int)]
         lib.qpb_modulus_project.argtypes = [POINTER(Problem), c_void_p, c_int, POINTER(c_float)]
+        lib.qpb_modulus_project_noalloc.argtypes = [c_int, POINTER(c_int64), c_void_p, c_void_p,
+                                                    c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_support_project.argtypes = [c_void_p, c_void_p, c_size_t]
         lib.qpb_gaussian_blur.argtypes = [c_void_p, c_int, POINTER(c_int64), c_float, c_void_p]
         _lib = lib

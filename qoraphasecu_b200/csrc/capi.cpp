@@ -78,6 +78,11 @@ void use_solver_device(const qpb_solver* solver) {
 
 }  // namespace
 
+namespace qpb {
+void set_last_error(const char* message) { g_last_error = message; }
+void clear_last_error() { g_last_error.clear(); }
+}  // namespace qpb
+
 extern "C" {
 
 const char* qpb_last_error(void) { return g_last_error.c_str(); }

@@ -83,6 +83,10 @@ inline void cuda_check(cudaError_t status, const char* what) {
 void count_launches(unsigned long long n);
 unsigned long long launches();
 
+// The thread-local message qpb_last_error() returns.
+void set_last_error(const char* message);
+void clear_last_error();
+
 // Host-side trace to stderr when the environment sets QPB_TRACE=1.
 bool tracing();
 void trace(const char* fmt, ...) __attribute__((format(printf, 1, 2)));

@@ -1,0 +1,198 @@
+// Modulus projection that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: applications that reserve their whole
+// GPU memory budget up front (a detector's streaming pipeline, a service whose
+// memory pool already owns most of HBM) and must not grow it later, and
+// latency-sensitive host threads for which cudaMalloc's implicit device
+// synchronisation is not acceptable. For them, this file keeps the scratch the
+// projection needs (signed amplitude, twiddle tables, control block, error
+// accumulators) in one file-scope __device__ array of fixed size, and the
+// caller passes every input and output as device memory.
+//
+// Limits: at most kNoAllocMaxElements elements per array, at most
+// kNoAllocMaxLine along any axis. The array is shared by every call on a
+// device and keeps the last call's contents; calls that overlap on the GPU
+// race on it.
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "../../include/qpb.h"
+#include "fft_plan.hpp"
+#include "line_pass.cuh"
+#include "reduce.cuh"
+
+namespace qpb {
+
+namespace {
+
+constexpr long long kNoAllocMaxElements = 65536;  // e.g. 256 x 256 or 40 x 40 x 40
+constexpr int kNoAllocMaxLine = 4096;
+
+// Byte layout of the scratch array.
+constexpr std::size_t kCtrlOffset = 0;       // Ctrl
+constexpr std::size_t kCounterOffset = 64;   // int
+constexpr std::size_t kErrOffset = 128;      // double: Fourier-error numerator
+constexpr std::size_t kEnergyOffset = 136;   // double: usable energy
+constexpr std::size_t kTwiddleOffset = 256;  // 3 axes x kNoAllocMaxLine float2
+constexpr std::size_t kAmpOffset = kTwiddleOffset + 3 * kNoAllocMaxLine * sizeof(float2);
+constexpr std::size_t kScratchBytes = kAmpOffset + kNoAllocMaxElements * sizeof(float);
+static_assert(sizeof(Ctrl) <= kCounterOffset, "control block overlaps the counter");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+// Device address of the scratch array, looked up once per device. In host
+// code `g_noalloc_scratch` is only a stand-in for the symbol, never an address.
+unsigned char* scratch_address() {
+  static std::mutex mutex;
+  static std::map<int, unsigned char*> addresses;
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  auto it = addresses.find(device);
+  if (it != addresses.end()) return it->second;
+  void* ptr = nullptr;
+  QPB_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+  configure_line_passes();
+  return addresses.emplace(device, static_cast<unsigned char*>(ptr)).first->second;
+}
+
+// Resets the control block and the accumulators a call starts from.
+__global__ void reset_kernel(unsigned char* base) {
+  auto* ctrl = reinterpret_cast<Ctrl*>(base + kCtrlOffset);
+  auto* counter = reinterpret_cast<int*>(base + kCounterOffset);
+  *counter = 0;
+  *reinterpret_cast<double*>(base + kErrOffset) = 0.0;
+  *reinterpret_cast<double*>(base + kEnergyOffset) = 0.0;
+  ctrl->errs = reinterpret_cast<double*>(base + kErrOffset);
+  ctrl->capacity = 1;
+  ctrl->a = 0.0f;
+  ctrl->b = 0.0f;
+  ctrl->counters = counter;
+}
+
+// W_L^k = exp(-2 pi i k / L) from double-precision sincospi, rounded once.
+__global__ void twiddle_kernel(float2* tw, int length) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < length; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * static_cast<double>(k) / static_cast<double>(length), &s, &c);
+    tw[k] = {static_cast<float>(c), static_cast<float>(s)};
+  }
+}
+
+// Signed amplitude (-1 on masked pixels) and the usable energy sum(A^2).
+__global__ void signed_amplitude_kernel(const float* amp, const std::uint8_t* mask, float* out,
+                                        long long n, double* energy) {
+  double e = 0.0;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const bool masked = mask && mask[i];
+    const float a = amp[i];
+    out[i] = masked ? -1.0f : a;
+    if (!masked) e += static_cast<double>(a) * a;
+  }
+  e = block_sum_double(e);
+  if (threadIdx.x == 0) atomicAdd(energy, e);
+}
+
+__global__ void finalize_kernel(const double* num, const double* energy, float* error_out) {
+  *error_out = static_cast<float>(sqrt(*num / (*energy + static_cast<double>(kEps))));
+}
+
+void check_launch() {
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+}  // namespace
+
+}  // namespace qpb
+
+extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape,
+                                                  const float* amplitude, const uint8_t* mask,
+                                                  const float* x, float* out, float* error_out,
+                                                  void* stream) {
+  using namespace qpb;
+  try {
+    clear_last_error();
+    if (!shape || !amplitude || !x || !out || !error_out) {
+      throw InvalidArgument("NULL argument");
+    }
+    if (ndim != 2 && ndim != 3) {
+      throw InvalidArgument("shape must be 2D or 3D, got ndim=" + std::to_string(ndim));
+    }
+    int dims[3] = {1, 1, 1};
+    long long n = 1;
+    for (int a = 0; a < ndim; ++a) {
+      if (shape[a] < 1) throw InvalidArgument("shape has a zero-length axis");
+      if (shape[a] > kNoAllocMaxLine) {
+        throw InvalidArgument("qpb_modulus_project_noalloc: axis length " +
+                              std::to_string(shape[a]) + " exceeds its maximum of " +
+                              std::to_string(kNoAllocMaxLine));
+      }
+      dims[3 - ndim + a] = static_cast<int>(shape[a]);
+      n *= shape[a];
+    }
+    if (n > kNoAllocMaxElements) {
+      throw InvalidArgument("qpb_modulus_project_noalloc: " + std::to_string(n) +
+                            " elements exceed its maximum of " +
+                            std::to_string(kNoAllocMaxElements));
+    }
+    const auto s = static_cast<cudaStream_t>(stream);
+    unsigned char* base = scratch_address();
+    auto* ctrl = reinterpret_cast<Ctrl*>(base + kCtrlOffset);
+    auto* twiddles = reinterpret_cast<float2*>(base + kTwiddleOffset);
+    auto* signed_amp = reinterpret_cast<float*>(base + kAmpOffset);
+
+    reset_kernel<<<1, 1, 0, s>>>(base);
+    check_launch();
+    const int first_axis = ndim == 2 ? 1 : 0;
+    PassParams axis_params[3] = {};
+    for (int a = first_axis; a < 3; ++a) {
+      const int L = dims[a];
+      const auto radices = factorize(L);
+      float2* tw = twiddles + a * kNoAllocMaxLine;
+      twiddle_kernel<<<(L + 255) / 256, 256, 0, s>>>(tw, L);
+      check_launch();
+      PassParams& p = axis_params[a];
+      p.w = reinterpret_cast<float2*>(out);
+      p.x = const_cast<float2*>(reinterpret_cast<const float2*>(x));
+      p.amp = signed_amp;
+      p.ctrl = ctrl;
+      p.twiddle = tw;
+      p.n = n;
+      p.L = L;
+      p.S = a == 2 ? 1 : a == 1 ? dims[2] : dims[1] * dims[2];
+      p.lines_per_start = static_cast<int>(n / L);
+      p.lines = p.lines_per_start;
+      p.lpc = choose_lpc(L, p.S, p.lines_per_start);
+      p.stages = static_cast<int>(radices.size());
+      for (int k = 0; k < p.stages; ++k) p.radix[k] = radices[k];
+      p.scale = 1.0f / std::sqrt(static_cast<float>(n));
+      p.starts_total = 1;
+      p.amp_storage = AmpStorage::kF32;
+    }
+    signed_amplitude_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, s>>>(
+        amplitude, mask, signed_amp, n, reinterpret_cast<double*>(base + kEnergyOffset));
+    check_launch();
+    // Forward transform into `out`, modulus with the error, inverse in place.
+    launch_line_pass(Mode::kFwdFromX, axis_params[2], s);
+    if (ndim == 3) launch_line_pass(Mode::kFwd, axis_params[1], s);
+    launch_line_pass(Mode::kMod, axis_params[first_axis], s);
+    if (ndim == 3) launch_line_pass(Mode::kInv, axis_params[1], s);
+    launch_line_pass(Mode::kInv, axis_params[2], s);
+    finalize_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const double*>(base + kErrOffset),
+                                    reinterpret_cast<const double*>(base + kEnergyOffset),
+                                    error_out);
+    check_launch();
+    return QPB_OK;
+  } catch (const std::invalid_argument& e) {
+    set_last_error(e.what());
+    return QPB_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return QPB_RUNTIME_ERROR;
+  }
+}
