@@ -198,6 +198,24 @@ def run_reference(args):
     return 0
 
 
+def run_profile(iterations):
+    """The benchmark workload cut to a few iterations launched directly (no graph),
+    so that an ncu capture sees each line pass of the timed loop after a short
+    set-up: make_problem, solver construction, `iterations` RAAR iterations."""
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+    from qoraphasecu_b200.recipe import RAAR, Recipe
+
+    _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
+    problem = qpc.make_problem(intensity, mask=mask)
+    with qpc.Solver(problem, starts=STARTS, seed=0, variant="batched", sync_every=1) as solver:
+        solver.run(Recipe(RAAR(iterations, 0.9)))
+        print(json.dumps({"profile_iterations": iterations,
+                          "kernels": qpc.kernel_launches(),
+                          "final_errors": [float(r.error) for r in solver.results()[:4]]}))
+    return 0
+
+
 # ---------------------------------------------------------------------- our arm
 def main(argv=None):
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
@@ -209,7 +227,11 @@ def main(argv=None):
     parser.add_argument("--cpu-seconds", type=float, default=10.0)
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
+    parser.add_argument("--profile", type=int, default=0, metavar="ITERS",
+                        help="only build the workload and run ITERS RAAR iterations (for ncu)")
     args = parser.parse_args(argv)
+    if args.profile:
+        return run_profile(args.profile)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -29,6 +29,9 @@ qpb_status guarded(F&& f) {
   } catch (const std::invalid_argument& e) {
     g_last_error = e.what();
     return QPB_INVALID_ARGUMENT;
+  } catch (const qpb::Timeout& e) {
+    g_last_error = e.what();
+    return QPB_TIMEOUT;
   } catch (const std::exception& e) {
     g_last_error = e.what();
     return QPB_RUNTIME_ERROR;

@@ -70,6 +70,11 @@ struct InvalidArgument : std::invalid_argument {
   using std::invalid_argument::invalid_argument;
 };
 
+// A kernel's bounded wait gave up (QPB_TIMEOUT at the C ABI).
+struct Timeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 inline void cuda_check(cudaError_t status, const char* what) {
   if (status != cudaSuccess) {
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(status));

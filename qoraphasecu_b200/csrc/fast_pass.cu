@@ -1,0 +1,548 @@
+// Register-resident line passes for power-of-two line lengths 16..1024.
+//
+// A line of length L is held by T = L / E threads, E complex values each, in
+// the "stride-T" distribution: thread t owns elements t + T m, m < E. Every
+// Stockham stage of radix R (<= E) is E / R butterflies per thread on
+// registers; between stages the values go once through shared memory (written
+// at their Stockham output positions, read back in the stride-T
+// distribution). The last stage's outputs already sit in the stride-T
+// distribution, so a 256-point transform (16 x 16) costs one shared-memory
+// round trip and an inverse transform can start from the forward's registers.
+//
+// Rows (stride 1) map 16..256 lines to a CTA, threads of a line adjacent;
+// columns (stride S) map adjacent lines to adjacent threads, so a half-warp
+// reads 16 neighbouring elements of one row either way (128-byte segments).
+// Shared-memory lines are padded (one slot per 16, pitch = 1 mod 16) so the
+// Stockham writes and the stride-T reads are free of bank conflicts.
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <set>
+#include <stdexcept>
+
+#include "bulk_copy.cuh"
+#include "butterfly.cuh"
+#include "fast_pass.cuh"
+#include "reduce.cuh"
+
+namespace qpb {
+
+namespace {
+
+__host__ __device__ constexpr int swz(int i) { return i + (i >> 4); }
+
+template <int L>
+struct Geometry {
+  static constexpr int E = L == 32 || L == 64 ? 8 : 16;
+  static constexpr int T = L / E;
+  static constexpr int LINES = T <= 16 ? 256 / T : (L >= 1024 ? 8 : 16);
+  static constexpr int NT = T * LINES;
+  // CTAs per SM the register budget is sized for (registers <= 64K / (NT * MIN_CTAS)).
+  static constexpr int MIN_CTAS = NT <= 256 ? 3 : 1;
+  // Radix of each stage (product = L, each <= E).
+  static constexpr int R0 = L <= 16 ? L : E;
+  static constexpr int R1 = L <= 16 ? 1 : (L / R0 <= E ? L / R0 : E);
+  static constexpr int R2 = L / (R0 * R1);
+  static constexpr int STAGES = L <= 16 ? 1 : (R2 == 1 ? 2 : 3);
+  static constexpr int PITCH = swz(L) + 1;
+  static constexpr int SMEM = STAGES > 1 ? LINES * PITCH * 8 : 0;
+  static_assert(R0 * R1 * R2 == L, "bad factorisation");
+  static_assert(R2 <= E && R1 <= E, "radix above the register count");
+};
+
+template <int R, bool INV>
+__device__ __forceinline__ void butterfly(float2* u) {
+  if constexpr (R == 2) {
+    bfly2<INV>(u[0], u[1]);
+  } else if constexpr (R == 4) {
+    bfly4<INV>(u[0], u[1], u[2], u[3]);
+  } else if constexpr (R == 8) {
+    bfly8<INV>(u);
+  } else if constexpr (R == 16) {
+    bfly16<INV>(u);
+  }
+}
+
+// One Stockham stage of radix R over the thread's E registers. NS is the
+// product of the radices before it; LAST stages leave values in place,
+// others exchange through the line's shared-memory row.
+template <int L, int R, int NS, bool LAST, bool INV>
+__device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
+                                      const float2* __restrict__ tw, float2* row) {
+  using G = Geometry<L>;
+  constexpr int E = G::E;
+  constexpr int T = G::T;
+  constexpr int Q = E / R;
+  constexpr int STEP = L / (NS * R);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    float2 u[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
+    const int j = t + T * q;
+    const int k = j & (NS - 1);
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = __ldg(tw + r * k * STEP);
+        u[r] = INV ? cmulc(u[r], w) : cmul(u[r], w);
+      }
+    }
+    butterfly<R, INV>(u);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q + r * Q] = u[r];
+    } else {
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[swz(base + r * NS)] = u[r];
+    }
+  }
+  if constexpr (!LAST) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = row[swz(t + T * m)];
+    __syncthreads();
+  }
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
+                                          const float2* __restrict__ tw, float2* row) {
+  using G = Geometry<L>;
+  if constexpr (G::STAGES == 1) {
+    stage<L, G::R0, 1, true, INV>(v, t, tw, row);
+  } else if constexpr (G::STAGES == 2) {
+    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
+    stage<L, G::R1, G::R0, true, INV>(v, t, tw, row);
+  } else {
+    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
+    stage<L, G::R1, G::R0, false, INV>(v, t, tw, row);
+    stage<L, G::R2, G::R0 * G::R1, true, INV>(v, t, tw, row);
+  }
+}
+
+template <class AmpT>
+__device__ __forceinline__ float to_float(AmpT a) {
+  if constexpr (std::is_same_v<AmpT, float>) {
+    return a;
+  } else if constexpr (std::is_same_v<AmpT, __half>) {
+    return __half2float(a);
+  } else {
+    return __bfloat162float(a);
+  }
+}
+
+// Bounded waits that gave up (read and cleared by take_fast_wait_failures).
+__device__ int g_fast_wait_failures = 0;
+
+__host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 * 16; }
+
+// Shared-memory layout of one CTA: the Stockham exchange rows, then the side
+// inputs staged by bulk copies (the amplitude tile of a modulus pass; the
+// old-iterate and support tiles of a row update pass), then the mbarrier.
+template <int L, bool ROWS, Mode M, class AmpT>
+struct Staging {
+  using G = Geometry<L>;
+  static constexpr bool kAmp = M == Mode::kMod;
+  static constexpr bool kUpd = M == Mode::kUpd && ROWS;
+  static constexpr int kExchange = align16(G::SMEM);
+  static constexpr int kSideA =
+      kAmp ? G::LINES * L * static_cast<int>(sizeof(AmpT)) : (kUpd ? G::LINES * L * 8 : 0);
+  static constexpr int kSideB = kUpd ? G::LINES * L : 0;
+  static constexpr int kBarrier = align16(kExchange + kSideA + kSideB);
+  static constexpr int kBytes = (kAmp || kUpd) ? kBarrier + 16 : G::SMEM;
+  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0, "bulk copies need 16-byte sizes");
+};
+
+template <int L, bool ROWS, Mode M, class AmpT>
+__global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_pass_kernel(const PassParams p) {
+  using G = Geometry<L>;
+  constexpr int E = G::E;
+  constexpr int T = G::T;
+  extern __shared__ float2 smem[];
+  const int tid = threadIdx.x;
+  const int l = ROWS ? tid / T : tid % G::LINES;
+  const int t = ROWS ? tid % T : tid / G::LINES;
+  float2* row = smem + l * G::PITCH;
+
+  const long long line0 = static_cast<long long>(blockIdx.x) * G::LINES;
+  const int batch_start = static_cast<int>(line0 / p.lines_per_start);
+  const long long start_off = static_cast<long long>(batch_start) * p.n;
+  // Element t + T m of line (line0 + l) sits at base + (t + T m) * S; the
+  // offsets from the thread's first element fit 32 bits (L * S <= n).
+  long long base;
+  int step;  // distance between a thread's consecutive elements
+  if constexpr (ROWS) {
+    base = (line0 + l) * L + t;
+    step = T;
+  } else {
+    const long long outer = line0 / p.S;
+    const long long inner = line0 - outer * p.S + l;
+    base = outer * static_cast<long long>(L) * p.S + inner + static_cast<long long>(t) * p.S;
+    step = T * p.S;
+  }
+  float2* __restrict__ wl = p.w + base;
+  float2* __restrict__ xl = p.x + base;
+  const float2* __restrict__ tw = p.twiddle;
+
+  // Side inputs that do not depend on the transform (the amplitude tile of a
+  // modulus pass, the old iterate and support of a row update) are copied to
+  // shared memory by bulk asynchronous copies issued now, so they arrive while
+  // the wave is loaded and transformed and hold no registers.
+  using St = Staging<L, ROWS, M, AmpT>;
+  unsigned char* sbase = reinterpret_cast<unsigned char*>(smem);
+  [[maybe_unused]] auto* bar = reinterpret_cast<std::uint64_t*>(sbase + St::kBarrier);
+  if constexpr (St::kAmp || St::kUpd) {
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      mbar_arrive_expect_tx(bar, St::kSideA + St::kSideB);
+    }
+    __syncthreads();
+    if constexpr (St::kUpd) {
+      if (tid == 0) {
+        bulk_g2s(sbase + St::kExchange, p.x + line0 * L, St::kSideA, bar);
+        bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, bar);
+      }
+    } else if (ROWS || p.amp_tiled) {
+      // FFT-order rows, or the amplitude pre-tiled in this pass's CTA order:
+      // the CTA's tile is one contiguous block.
+      if (tid == 0) {
+        const long long line_in_start = line0 - static_cast<long long>(batch_start) * p.lines_per_start;
+        const AmpT* src = static_cast<const AmpT*>(p.amp) + line_in_start * L;
+        bulk_g2s(sbase + St::kExchange, src, St::kSideA, bar);
+      }
+    } else {
+      // one copy per element index j of the lines: LINES adjacent amplitudes
+      const long long outer = line0 / p.S;
+      const AmpT* src = static_cast<const AmpT*>(p.amp) +
+                        (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
+      constexpr int kRowBytes = G::LINES * static_cast<int>(sizeof(AmpT));
+      for (int j = tid; j < L; j += G::NT) {
+        bulk_g2s(sbase + St::kExchange + j * kRowBytes, src + static_cast<long long>(j) * p.S,
+                 kRowBytes, bar);
+      }
+    }
+  }
+
+  float2 v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    if constexpr (M == Mode::kFwdFromX) {
+      v[m] = xl[m * step];
+    } else if constexpr (M == Mode::kBlurMag) {
+      const float2 xv = xl[m * step];
+      v[m] = {sqrtf(xv.x * xv.x + xv.y * xv.y), 0.0f};
+    } else {
+      v[m] = wl[m * step];
+    }
+  }
+
+  constexpr bool kStartsInverse = M == Mode::kInv || M == Mode::kUpd;
+  transform<L, kStartsInverse>(v, t, tw, row);
+
+  if constexpr (St::kAmp || St::kUpd) {
+    // Every thread waits (bounded); if any gave up, the CTA records it and
+    // leaves together, writing nothing.
+    if (!__syncthreads_and(mbar_wait(bar, 0) ? 1 : 0)) {
+      if (tid == 0) atomicAdd(&g_fast_wait_failures, 1);
+      return;
+    }
+  }
+
+  if constexpr (M == Mode::kMod) {
+    const float s = p.scale;
+    float acc = 0.0f;
+    const AmpT* amp_tile = reinterpret_cast<const AmpT*>(sbase + St::kExchange);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int j = t + T * m;
+      const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * G::LINES + l]);
+      const float re = v[m].x * s;
+      const float im = v[m].y * s;
+      const float mag = sqrtf(re * re + im * im);
+      float target = mag;
+      if (a >= 0.0f) {
+        const float d = mag - a;
+        acc += d * d;
+        target = a;
+      }
+      // approximate division (<= 2 ulp): branch-free, far inside the tolerance
+      const float f = __fdividef(target, mag + kEps) * s;
+      v[m] = {re * f, im * f};
+    }
+    const double total = block_sum_double(static_cast<double>(acc));
+    if (tid == 0) {
+      Ctrl* c = p.ctrl;
+      const int r = c->counters[p.group];
+      if (r < c->capacity) {
+        atomicAdd(&c->errs[static_cast<long long>(r) * p.starts_total + p.start0 + batch_start],
+                  total);
+      }
+    }
+    transform<L, true>(v, t, tw, row);
+  } else if constexpr (M == Mode::kUpd) {
+    float ca = p.coef_a, cb = p.coef_b;
+    if (p.coef_from_ctrl) {
+      ca = p.ctrl->a;
+      cb = p.ctrl->b;
+    }
+    if constexpr (St::kUpd) {
+      const float2* x_tile = reinterpret_cast<const float2*>(sbase + St::kExchange);
+      const std::uint8_t* s_tile = sbase + St::kExchange + St::kSideA;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int j = l * L + t + T * m;
+        float2 xn = v[m];
+        if (!s_tile[j]) {
+          const float2 xo = x_tile[j];
+          xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
+        }
+        xl[m * step] = xn;
+        v[m] = xn;
+      }
+    } else {
+      const std::uint8_t* __restrict__ sl = p.support + base;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        float2 xn = v[m];
+        if (!sl[m * step]) {
+          const float2 xo = xl[m * step];
+          xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
+        }
+        xl[m * step] = xn;
+        v[m] = xn;
+      }
+    }
+    if (p.bump_counter && blockIdx.x == 0 && tid == 0) ++p.ctrl->counters[p.group];
+    __syncthreads();
+    transform<L, false>(v, t, tw, row);
+  } else if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
+    const float inv_l = 1.0f / static_cast<float>(L);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int j = t + T * m;
+      const float f = fftfreq(static_cast<std::uint32_t>(j), static_cast<std::uint32_t>(L));
+      v[m] = cscale(v[m], expf(p.blur_k * f * f) * inv_l);
+    }
+    transform<L, true>(v, t, tw, row);
+  }
+
+  float peak = 0.0f;
+  float sq = 0.0f;
+  unsigned cnt = 0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    wl[m * step] = v[m];
+    if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
+      if (p.level_method == 1) {
+        peak = fmaxf(peak, v[m].x);
+      } else if (p.level_method == 2 && p.support[base + m * step]) {
+        sq += v[m].x * v[m].x;
+        ++cnt;
+      }
+    }
+  }
+  if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
+    if (p.level_method == 1) {
+      peak = warp_max(peak);
+      if ((tid & 31) == 0) atomicMax(&p.level[batch_start].max_bits, __float_as_int(peak));
+    } else if (p.level_method == 2) {
+      const double s2 = block_sum_double(static_cast<double>(sq));
+      __syncthreads();
+      const double c2 = block_sum_double(static_cast<double>(cnt));
+      if (tid == 0) {
+        atomicAdd(&p.level[batch_start].sum, s2);
+        atomicAdd(&p.level[batch_start].count, static_cast<unsigned long long>(c2));
+      }
+    }
+  }
+}
+
+template <int L, bool ROWS, Mode M, class AmpT>
+void launch_one(const PassParams& p, cudaStream_t stream) {
+  using G = Geometry<L>;
+  const dim3 grid(static_cast<unsigned>(p.lines / G::LINES));
+  fast_pass_kernel<L, ROWS, M, AmpT>
+      <<<grid, G::NT, Staging<L, ROWS, M, AmpT>::kBytes, stream>>>(p);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+template <int L, bool ROWS, Mode M>
+void launch_storage(const PassParams& p, cudaStream_t stream) {
+  if constexpr (M == Mode::kMod) {
+    switch (p.amp_storage) {
+      case AmpStorage::kF32:
+        return launch_one<L, ROWS, M, float>(p, stream);
+      case AmpStorage::kF16:
+        return launch_one<L, ROWS, M, __half>(p, stream);
+      case AmpStorage::kBF16:
+        return launch_one<L, ROWS, M, __nv_bfloat16>(p, stream);
+    }
+  } else {
+    launch_one<L, ROWS, M, float>(p, stream);
+  }
+}
+
+template <int L, bool ROWS>
+void launch_mode(Mode mode, const PassParams& p, cudaStream_t stream) {
+  switch (mode) {
+    case Mode::kFwd:
+      return launch_storage<L, ROWS, Mode::kFwd>(p, stream);
+    case Mode::kFwdFromX:
+      return launch_storage<L, ROWS, Mode::kFwdFromX>(p, stream);
+    case Mode::kInv:
+      return launch_storage<L, ROWS, Mode::kInv>(p, stream);
+    case Mode::kMod:
+      return launch_storage<L, ROWS, Mode::kMod>(p, stream);
+    case Mode::kUpd:
+      return launch_storage<L, ROWS, Mode::kUpd>(p, stream);
+    case Mode::kBlur:
+      return launch_storage<L, ROWS, Mode::kBlur>(p, stream);
+    case Mode::kBlurMag:
+      return launch_storage<L, ROWS, Mode::kBlurMag>(p, stream);
+  }
+}
+
+template <int L>
+void launch_length(Mode mode, const PassParams& p, cudaStream_t stream) {
+  if (p.S == 1) {
+    launch_mode<L, true>(mode, p, stream);
+  } else {
+    launch_mode<L, false>(mode, p, stream);
+  }
+}
+
+template <int L>
+int lines_per_cta() {
+  return Geometry<L>::LINES;
+}
+
+int fast_lines(int L) {
+  switch (L) {
+    case 16: return lines_per_cta<16>();
+    case 32: return lines_per_cta<32>();
+    case 64: return lines_per_cta<64>();
+    case 128: return lines_per_cta<128>();
+    case 256: return lines_per_cta<256>();
+    case 512: return lines_per_cta<512>();
+    case 1024: return lines_per_cta<1024>();
+    default: return 0;
+  }
+}
+
+template <int L, bool ROWS, Mode M, class AmpT>
+void allow_smem_one() {
+  constexpr int bytes = Staging<L, ROWS, M, AmpT>::kBytes;
+  if constexpr (bytes > 48 * 1024) {
+    QPB_CHECK(cudaFuncSetAttribute(fast_pass_kernel<L, ROWS, M, AmpT>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  }
+}
+
+template <int L, bool ROWS>
+void allow_smem_modes() {
+  allow_smem_one<L, ROWS, Mode::kFwd, float>();
+  allow_smem_one<L, ROWS, Mode::kFwdFromX, float>();
+  allow_smem_one<L, ROWS, Mode::kInv, float>();
+  allow_smem_one<L, ROWS, Mode::kMod, float>();
+  allow_smem_one<L, ROWS, Mode::kMod, __half>();
+  allow_smem_one<L, ROWS, Mode::kMod, __nv_bfloat16>();
+  allow_smem_one<L, ROWS, Mode::kUpd, float>();
+  allow_smem_one<L, ROWS, Mode::kBlur, float>();
+  allow_smem_one<L, ROWS, Mode::kBlurMag, float>();
+}
+
+template <int L>
+void allow_smem_length() {
+  allow_smem_modes<L, true>();
+  allow_smem_modes<L, false>();
+}
+
+}  // namespace
+
+void configure_fast_passes() {
+  static std::mutex mutex;
+  static std::set<int> done;
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  if (!done.insert(device).second) return;
+  allow_smem_length<16>();
+  allow_smem_length<32>();
+  allow_smem_length<64>();
+  allow_smem_length<128>();
+  allow_smem_length<256>();
+  allow_smem_length<512>();
+  allow_smem_length<1024>();
+}
+
+bool fast_passes_enabled() {
+  static const bool enabled = [] {
+    const char* v = std::getenv("QPB_GENERIC_PASSES");
+    return !(v && *v && *v != '0');
+  }();
+  return enabled;
+}
+
+int fast_pass_lines(const PassParams& p) {
+  return fast_passes_enabled() && fast_pass_supports(p) ? fast_lines(p.L) : 0;
+}
+
+std::vector<unsigned char> tile_amplitude(const std::vector<unsigned char>& amp,
+                                          std::size_t elem_size, long long n, int L, int S,
+                                          int lines) {
+  if (S == 1) return amp;  // rows: FFT order already has each CTA's lines contiguous
+  std::vector<unsigned char> out(amp.size());
+  const long long slab = static_cast<long long>(L) * S;
+  for (long long e = 0; e < n; ++e) {
+    const long long outer = e / slab;
+    const long long rem = e - outer * slab;
+    const long long j = rem / S;
+    const long long col = rem - j * S;
+    const long long tile = outer * (S / lines) + col / lines;
+    const long long c = col % lines;
+    const long long to = S > 1 ? (tile * L + j) * lines + c : (tile * lines + c) * L + j;
+    std::memcpy(&out[to * elem_size], &amp[e * elem_size], elem_size);
+  }
+  return out;
+}
+
+int take_fast_wait_failures() {
+  int failures = 0;
+  QPB_CHECK(cudaMemcpyFromSymbol(&failures, g_fast_wait_failures, sizeof(int)));
+  if (failures) {
+    const int zero = 0;
+    QPB_CHECK(cudaMemcpyToSymbol(g_fast_wait_failures, &zero, sizeof(int)));
+  }
+  return failures;
+}
+
+bool fast_pass_supports(const PassParams& p) {
+  const int lines = fast_lines(p.L);
+  if (lines == 0) return false;
+  if (p.lines_per_start % lines != 0 || p.lines % lines != 0) return false;
+  // Columns: the CTA's lines must be adjacent within one outer slab.
+  if (p.S != 1 && p.S % lines != 0) return false;
+  return true;
+}
+
+void launch_fast_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
+  switch (p.L) {
+    case 16: return launch_length<16>(mode, p, stream);
+    case 32: return launch_length<32>(mode, p, stream);
+    case 64: return launch_length<64>(mode, p, stream);
+    case 128: return launch_length<128>(mode, p, stream);
+    case 256: return launch_length<256>(mode, p, stream);
+    case 512: return launch_length<512>(mode, p, stream);
+    case 1024: return launch_length<1024>(mode, p, stream);
+    default: throw std::logic_error("fast line pass: unsupported length");
+  }
+}
+
+}  // namespace qpb

@@ -10,11 +10,13 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <set>
 #include <stdexcept>
 
 #include "butterfly.cuh"
+#include "fast_pass.cuh"
 #include "line_pass.cuh"
 #include "reduce.cuh"
 
@@ -355,6 +357,7 @@ void configure_line_passes() {
   allow_smem(line_pass_kernel<Mode::kUpd, float>);
   allow_smem(line_pass_kernel<Mode::kBlur, float>);
   allow_smem(line_pass_kernel<Mode::kBlurMag, float>);
+  configure_fast_passes();
 }
 
 int choose_lpc(int L, int S, int lines_per_start) {
@@ -368,6 +371,8 @@ int choose_lpc(int L, int S, int lines_per_start) {
 }
 
 void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
+  if (fast_passes_enabled() && fast_pass_supports(p)) return launch_fast_pass(mode, p, stream);
+  if (p.amp_tiled) throw std::logic_error("line pass: tiled amplitude needs the register-resident pass");
   if (p.lines % p.lpc != 0 || p.lines_per_start % p.lpc != 0) {
     throw std::logic_error("line pass: lines per CTA must divide the lines of a start");
   }

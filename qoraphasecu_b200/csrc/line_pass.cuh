@@ -75,6 +75,9 @@ struct PassParams {
   int coef_from_ctrl;
   int bump_counter;               // kUpd increments ctrl->counters[group]
   AmpStorage amp_storage;
+  // The amplitude is stored in the CTA order of a register-resident modulus
+  // pass (tile_amplitude) instead of FFT order: one contiguous tile per CTA.
+  int amp_tiled;
 };
 
 // Launches one generic line pass on `stream`.

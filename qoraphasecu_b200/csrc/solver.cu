@@ -14,6 +14,7 @@
 #include <cstring>
 #include <string>
 
+#include "fast_pass.cuh"
 #include "solver.hpp"
 
 namespace qpb {
@@ -63,6 +64,14 @@ void trace(const char* fmt, ...) {
   std::fputc('\n', stderr);
   std::fflush(stderr);
   va_end(args);
+}
+
+// Throws Timeout when a kernel's bounded wait gave up since the last check.
+void check_waits() {
+  if (const int failed = take_fast_wait_failures()) {
+    throw Timeout(std::to_string(failed) +
+                  " line-pass CTAs gave up waiting for their staged inputs; results are invalid");
+  }
 }
 
 namespace {
@@ -261,7 +270,20 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   auto sup = host_roll(problem.support, d_, true);
   for (auto& s : sup) s = s != 0;
   energy_ = usable_energy(amp, mask);
-  amp_ = upload(signed_amplitude(amp, mask, options.amp_storage), stream_);
+  {
+    // The amplitude is read by the modulus pass only; when that pass runs the
+    // register-resident kernel, store it in the kernel's CTA order so each CTA
+    // stages its tile with one bulk copy.
+    auto bytes = signed_amplitude(amp, mask, options.amp_storage);
+    const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
+    const int lines = fast_pass_lines(mod);
+    if (lines > 0 && mod.S > 1) {
+      const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
+      bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
+      amp_tiled_ = true;
+    }
+    amp_ = upload(bytes, stream_);
+  }
 
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
   x_ = DeviceBuffer<float2>(total);
@@ -331,6 +353,7 @@ PassParams Solver::base(Mode mode, int axis3, int g) const {
   p.coef_from_ctrl = 1;
   p.bump_counter = 1;
   p.amp_storage = options_.amp_storage;
+  p.amp_tiled = amp_tiled_ && mode == Mode::kMod ? 1 : 0;
   return p;
 }
 
@@ -400,6 +423,7 @@ void Solver::run(const OpDesc* ops, std::size_t count) {
     }
   }
   collect_errors(run_iterations_);
+  check_waits();
 }
 
 void Solver::iterate(int count, Coefficients c) {
@@ -636,6 +660,7 @@ float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storag
                             cudaMemcpyDeviceToHost, ctx.stream));
   QPB_CHECK(cudaMemcpyAsync(&num, errs.get(), sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
   ctx.stream.sync();
+  check_waits();
   const auto centred = host_roll(host.data(), d, false);
   std::copy(centred.begin(), centred.end(), obj);
   return static_cast<float>(std::sqrt(num / (energy + kEps)));
@@ -672,6 +697,7 @@ void gaussian_blur(const float* image, int ndim, const long long* shape, float s
   QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
                             cudaMemcpyDeviceToHost, ctx.stream));
   ctx.stream.sync();
+  check_waits();
   for (long long i = 0; i < n; ++i) out[i] = host[i].x;
 }
 
@@ -692,6 +718,7 @@ void autocorrelation_support(const float* intensity, int ndim, const long long* 
   QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
                             cudaMemcpyDeviceToHost, ctx.stream));
   ctx.stream.sync();
+  check_waits();
   // Unitary scale, |.|, centre-origin, threshold against the maximum.
   const float s = 1.0f / std::sqrt(static_cast<float>(n));
   std::vector<float> ac(static_cast<std::size_t>(n));

@@ -132,6 +132,9 @@ struct OpDesc {
 
 using ProgressFn = void (*)(void* user, int iteration, const float* errors, int count);
 
+// Throws Timeout when a kernel's bounded wait gave up since the last check.
+void check_waits();
+
 // Checks shape rank and extents; returns Dims3 (2D -> {1, ny, nx}).
 Dims3 dims_of(const ProblemView& p);
 void validate_recipe(const OpDesc* ops, std::size_t count);
@@ -216,6 +219,7 @@ class Solver {
   PassRunner runner_;
   double energy_ = 0.0;
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
+  bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
   DeviceBuffer<float2> x_;
   DeviceBuffer<float2> w_;
   DeviceBuffer<std::uint8_t> support_;

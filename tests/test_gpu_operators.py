@@ -43,6 +43,50 @@ def test_modulus_projection_matches_fp64(gpu, shape):
     assert again < 1e-5
 
 
+_GENERIC_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+import qoraphasecu_b200 as qpc
+from synthetic import random_field, triangle
+out = {{}}
+for shape in {shapes!r}:
+    _, support, intensity = triangle(shape, 8)
+    p = qpc.make_problem(intensity, support=support)
+    x = random_field(int(np.prod(shape)), 7).reshape(shape)
+    out["x".join(map(str, shape))] = qpc.modulus_project(p, x)[0]
+    out["blur" + "x".join(map(str, shape))] = qpc.gaussian_blur(np.abs(x), 1.3)
+np.savez({path!r}, **out)
+"""
+
+
+def test_register_resident_passes_match_the_generic_passes(gpu, tmp_path):
+    """The power-of-two kernels and the generic mixed-radix kernels compute the
+    same transforms (to FP32 rounding); the generic ones run in a child process
+    with QPB_GENERIC_PASSES=1."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    tests = Path(__file__).resolve().parent
+    shapes = [(16, 16), (32, 64), (64, 64), (128, 128), (256, 256), (512, 256), (1024, 16),
+              (16, 32, 64), (64, 64, 64)]
+    path = tmp_path / "generic.npz"
+    script = _GENERIC_SCRIPT.format(root=str(tests.parent), tests=str(tests), shapes=shapes,
+                                    path=str(path))
+    env = dict(os.environ, QPB_GENERIC_PASSES="1")
+    subprocess.run([sys.executable, "-c", script], check=True, env=env, timeout=600)
+    generic = np.load(path)
+    for shape in shapes:
+        _, support, intensity = triangle(shape, 8)
+        p = qpc.make_problem(intensity, support=support)
+        x = random_field(int(np.prod(shape)), 7).reshape(shape)
+        key = "x".join(map(str, shape))
+        assert fp64.relative_diff(qpc.modulus_project(p, x)[0], generic[key]) < 2e-6, shape
+        blur = qpc.gaussian_blur(np.abs(x), 1.3)
+        assert np.abs(blur - generic["blur" + key]).max() < 1e-5 * np.abs(blur).max(), shape
+
+
 def test_error_is_zero_at_the_true_object(gpu):
     obj, support, intensity = triangle((32, 32), 8)
     _, p = pair(intensity, support)
