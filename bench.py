@@ -216,6 +216,22 @@ def run_profile(iterations):
     return 0
 
 
+def run_profile_step(sync_every):
+    """One benchmark step (the whole recipe over 32 starts, tuned schedule)
+    after the solver is built, for an ncu launch list of the timed work."""
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+
+    _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
+    problem = qpc.make_problem(intensity, mask=mask)
+    with qpc.Solver(problem, starts=STARTS, seed=0, sync_every=sync_every) as solver:
+        before = qpc.kernel_launches()
+        solver.run(workloads.gaussians_recipe())
+        print(json.dumps({"step_kernels": qpc.kernel_launches() - before,
+                          "tuning": qpc.api.tuning_report().strip()}))
+    return 0
+
+
 # ---------------------------------------------------------------------- our arm
 def main(argv=None):
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
@@ -224,14 +240,20 @@ def main(argv=None):
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--sync-every", type=int, default=50)
+    parser.add_argument("--batch", type=int, default=0,
+                        help="starts per launch; groups run as parallel graph branches (0 = all)")
     parser.add_argument("--cpu-seconds", type=float, default=10.0)
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
     parser.add_argument("--profile", type=int, default=0, metavar="ITERS",
                         help="only build the workload and run ITERS RAAR iterations (for ncu)")
+    parser.add_argument("--profile-step", action="store_true",
+                        help="only build the workload and run one benchmark step (for ncu)")
     args = parser.parse_args(argv)
     if args.profile:
         return run_profile(args.profile)
+    if args.profile_step:
+        return run_profile_step(args.sync_every)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
@@ -274,7 +296,7 @@ def main(argv=None):
     stream = torch.cuda.current_stream()
     problem = qpc.make_problem(intensity, mask=mask)
     solver = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
-                        device=local, stream=stream.cuda_stream)
+                        batch=args.batch or None, device=local, stream=stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
@@ -300,8 +322,12 @@ def main(argv=None):
     total_ms = max_over_ranks(sum(step_ms))
     value = world * STARTS * iters * args.steps / (total_ms / 1e3)
 
-    # Per-pass device time (direct launches between events on the same stream).
-    pass_ms = solver.profile_passes(20)
+    # Per-kernel device time: every pass of an iteration launched directly
+    # between CUDA events on the same stream, all 32 starts in one launch.
+    with qpc.Solver(problem, starts=STARTS, seed=rank, batch=STARTS, device=local,
+                    stream=stream.cuda_stream) as single:
+        single.run(workloads.hio_recipe(5))
+        pass_ms = single.profile_passes(20)
     elems = STARTS * SHAPE[0] * SHAPE[1]
     passes = []
     for (name, bpe), ms in zip(PASS_BYTES.items(), pass_ms):
@@ -309,6 +335,11 @@ def main(argv=None):
     dominant = max(passes, key=lambda p: p["ms"])
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
+    # The whole iteration in the timed graph (parallel start groups, shrinkwrap
+    # amortised): minimum 21 B per element per iteration and the
+    # bytes the two fused passes move.
+    iter_ms = total_ms / args.steps / iters
+    fused_bytes = sum(PASS_BYTES.values()) * elems
     roofline = {
         "bound": "hbm",
         "kernel": dominant["pass"],
@@ -319,6 +350,13 @@ def main(argv=None):
         "frac": dominant["gbs"] / peak,
         "traffic": traffic,
         "passes": passes,
+        "iteration": {
+            "us": iter_ms * 1e3,
+            "min_bytes": 21 * elems,
+            "fused_pass_bytes": fused_bytes,
+            "achieved_min_gbs": 21 * elems / (iter_ms * 1e6),
+            "achieved_pass_gbs": fused_bytes / (iter_ms * 1e6),
+        },
         "note": "32 starts x 256^2 (16 MiB iterate) stay L2-resident across an iteration",
     }
 
@@ -341,11 +379,13 @@ def main(argv=None):
             "starts_per_gpu": STARTS,
             "iterations": iters,
             "variant": "batched, graph-captured",
+            "starts_per_launch": args.batch or STARTS,
             "sync_every": args.sync_every,
             "parallelism": f"replicas x{world}",
             "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write, outside step events)",
         },
         "gpu_launches": launches,
+        "tuning": qpc.api.tuning_report().strip().splitlines(),
         "wall_s_timed_region": wall_s,
         "roofline": roofline,
     }

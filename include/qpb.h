@@ -151,6 +151,12 @@ QPB_API void qpb_destroy(qpb_solver* solver);
  * launch count that bench.py reports. */
 QPB_API uint64_t qpb_kernel_launches(void);
 
+/* Writes the autotuner's choices so far (one line per tuned shape and start
+ * count: the starts per launch picked and the time of every candidate) into
+ * `out` (NUL-terminated, at most `len` bytes). No counterpart in the reference,
+ * which fixes the grouping through Options::batch (solver.hpp:44-46). */
+QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
+
 /* Runs `iterations` more iterations with every line pass launched directly
  * between CUDA events on the solver's stream; ms_out[p] receives the mean
  * duration of pass p of one iteration (2D: modulus pass, update pass; 3D adds

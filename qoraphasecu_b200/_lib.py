@@ -50,6 +50,7 @@ EXPORTS = (
     "qpb_results",
     "qpb_destroy",
     "qpb_kernel_launches",
+    "qpb_tuning_report",
     "qpb_profile_passes",
     "qpb_modulus_project_noalloc",
     "qpb_modulus_project",
@@ -138,6 +139,7 @@ def load():
         lib.qpb_kernel_launches.argtypes = []
         lib.qpb_kernel_launches.restype = c_uint64
         lib.qpb_profile_passes.argtypes = [c_void_p, c_int, POINTER(c_double), POINTER(c_int)]
+        lib.qpb_tuning_report.argtypes = [c_char_p, c_size_t]
         lib.qpb_modulus_project.argtypes = [POINTER(Problem), c_void_p, c_int, POINTER(c_float)]
         lib.qpb_modulus_project_noalloc.argtypes = [c_int, POINTER(c_int64), c_void_p, c_void_p,
                                                     c_void_p, c_void_p, c_void_p, c_void_p]

@@ -91,6 +91,13 @@ def set_device(device: int) -> None:
     _lib.check(_lib.load().qpb_set_device(device))
 
 
+def tuning_report() -> str:
+    """The autotuner's choices so far: starts per launch per shape and start count."""
+    buf = ctypes.create_string_buffer(8192)
+    _lib.check(_lib.load().qpb_tuning_report(buf, len(buf)))
+    return buf.value.decode()
+
+
 def kernel_launches() -> int:
     """Kernels libqpb.so has launched in this process (graph replays count each node)."""
     return int(_lib.load().qpb_kernel_launches())

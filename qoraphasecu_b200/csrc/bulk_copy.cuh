@@ -45,6 +45,30 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// Copies `bytes` (a multiple of 16) from shared `src` to global `dst`, both
+// 16-byte aligned, as part of this thread's current bulk group.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_addr(src)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Blocks until this thread's committed bulk stores have finished reading
+// shared memory (after which it may be reused or the CTA may exit).
+__device__ __forceinline__ void bulk_wait_reads() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory writes before later
+// asynchronous-proxy (bulk copy) reads of them.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, unsigned parity) {
   std::uint32_t done;
   asm volatile(

@@ -234,6 +234,15 @@ qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops) {
 
 uint64_t qpb_kernel_launches(void) { return qpb::launches(); }
 
+qpb_status qpb_tuning_report(char* out, size_t len) {
+  return guarded([&] {
+    require(out != nullptr && len > 0, "NULL argument");
+    const std::string report = qpb::tuning_report();
+    std::strncpy(out, report.c_str(), len - 1);
+    out[len - 1] = '\0';
+  });
+}
+
 qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes) {
   return guarded([&] {
     require(solver && ms_out && n_passes, "NULL argument");

@@ -142,26 +142,34 @@ __device__ int g_fast_wait_failures = 0;
 
 __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 * 16; }
 
-// Shared-memory layout of one CTA: the Stockham exchange rows, then the side
-// inputs staged by bulk copies (the amplitude tile of a modulus pass; the
-// old-iterate and support tiles of a row update pass), then the mbarrier.
+// Shared-memory layout of one CTA. Region W holds the Stockham exchange rows
+// and, for row passes that move whole tiles by bulk copies, the wave tile in
+// and out (its rows are contiguous in global memory); then the side inputs
+// staged by bulk copies (the amplitude tile of a modulus pass; the old-iterate
+// and support tiles of a row update); then the mbarrier.
 template <int L, bool ROWS, Mode M, class AmpT>
 struct Staging {
   using G = Geometry<L>;
+  static constexpr int kTile = G::LINES * L * 8;  // one complex64 tile
+  static constexpr bool kRowTma =
+      ROWS && (M == Mode::kFwd || M == Mode::kFwdFromX || M == Mode::kInv || M == Mode::kUpd);
   static constexpr bool kAmp = M == Mode::kMod;
   static constexpr bool kUpd = M == Mode::kUpd && ROWS;
-  static constexpr int kExchange = align16(G::SMEM);
+  static constexpr int kExchange = align16(kRowTma && kTile > G::SMEM ? kTile : G::SMEM);
   static constexpr int kSideA =
-      kAmp ? G::LINES * L * static_cast<int>(sizeof(AmpT)) : (kUpd ? G::LINES * L * 8 : 0);
+      kAmp ? G::LINES * L * static_cast<int>(sizeof(AmpT)) : (kUpd ? kTile : 0);
   static constexpr int kSideB = kUpd ? G::LINES * L : 0;
+  static constexpr bool kBarrierUsed = kAmp || kUpd || kRowTma;
   static constexpr int kBarrier = align16(kExchange + kSideA + kSideB);
-  static constexpr int kBytes = (kAmp || kUpd) ? kBarrier + 16 : G::SMEM;
-  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0, "bulk copies need 16-byte sizes");
+  static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : G::SMEM;
+  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTile % 16 == 0,
+                "bulk copies need 16-byte sizes");
 };
 
 template <int L, bool ROWS, Mode M, class AmpT>
 __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_pass_kernel(const PassParams p) {
   using G = Geometry<L>;
+  using St = Staging<L, ROWS, M, AmpT>;
   constexpr int E = G::E;
   constexpr int T = G::T;
   extern __shared__ float2 smem[];
@@ -190,68 +198,89 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
   float2* __restrict__ xl = p.x + base;
   const float2* __restrict__ tw = p.twiddle;
 
-  // Side inputs that do not depend on the transform (the amplitude tile of a
-  // modulus pass, the old iterate and support of a row update) are copied to
-  // shared memory by bulk asynchronous copies issued now, so they arrive while
-  // the wave is loaded and transformed and hold no registers.
-  using St = Staging<L, ROWS, M, AmpT>;
+  // Inputs that do not depend on the transform go to shared memory by bulk
+  // asynchronous copies issued first: the whole input tile of a row pass, the
+  // amplitude tile of a modulus pass, the old iterate and support of a row
+  // update. They hold no registers while in flight.
   unsigned char* sbase = reinterpret_cast<unsigned char*>(smem);
+  [[maybe_unused]] float2* wtile = smem;  // region W, rows of length L (bulk-copied passes)
   [[maybe_unused]] auto* bar = reinterpret_cast<std::uint64_t*>(sbase + St::kBarrier);
-  if constexpr (St::kAmp || St::kUpd) {
+  if constexpr (St::kBarrierUsed) {
     if (tid == 0) {
       mbar_init(bar, 1);
-      mbar_arrive_expect_tx(bar, St::kSideA + St::kSideB);
+      mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTile : 0) + St::kSideA + St::kSideB);
     }
     __syncthreads();
+    if constexpr (St::kRowTma) {
+      if (tid == 0) {
+        const float2* src = (M == Mode::kFwdFromX ? p.x : p.w) + line0 * L;
+        bulk_g2s(wtile, src, St::kTile, bar);
+      }
+    }
     if constexpr (St::kUpd) {
       if (tid == 0) {
         bulk_g2s(sbase + St::kExchange, p.x + line0 * L, St::kSideA, bar);
         bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, bar);
       }
-    } else if (ROWS || p.amp_tiled) {
-      // FFT-order rows, or the amplitude pre-tiled in this pass's CTA order:
-      // the CTA's tile is one contiguous block.
-      if (tid == 0) {
-        const long long line_in_start = line0 - static_cast<long long>(batch_start) * p.lines_per_start;
-        const AmpT* src = static_cast<const AmpT*>(p.amp) + line_in_start * L;
-        bulk_g2s(sbase + St::kExchange, src, St::kSideA, bar);
-      }
-    } else {
-      // one copy per element index j of the lines: LINES adjacent amplitudes
-      const long long outer = line0 / p.S;
-      const AmpT* src = static_cast<const AmpT*>(p.amp) +
-                        (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
-      constexpr int kRowBytes = G::LINES * static_cast<int>(sizeof(AmpT));
-      for (int j = tid; j < L; j += G::NT) {
-        bulk_g2s(sbase + St::kExchange + j * kRowBytes, src + static_cast<long long>(j) * p.S,
-                 kRowBytes, bar);
+    } else if constexpr (St::kAmp) {
+      if (ROWS || p.amp_tiled) {
+        // FFT-order rows, or the amplitude pre-tiled in this pass's CTA order:
+        // the CTA's tile is one contiguous block.
+        if (tid == 0) {
+          const long long line_in_start =
+              line0 - static_cast<long long>(batch_start) * p.lines_per_start;
+          const AmpT* src = static_cast<const AmpT*>(p.amp) + line_in_start * L;
+          bulk_g2s(sbase + St::kExchange, src, St::kSideA, bar);
+        }
+      } else {
+        // one copy per element index j of the lines: LINES adjacent amplitudes
+        const long long outer = line0 / p.S;
+        const AmpT* src = static_cast<const AmpT*>(p.amp) +
+                          (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
+        constexpr int kRowBytes = G::LINES * static_cast<int>(sizeof(AmpT));
+        for (int j = tid; j < L; j += G::NT) {
+          bulk_g2s(sbase + St::kExchange + j * kRowBytes, src + static_cast<long long>(j) * p.S,
+                   kRowBytes, bar);
+        }
       }
     }
   }
 
+  // Every thread waits (bounded); if any gave up, the CTA records it and
+  // leaves together, writing nothing.
+  auto staged = [&]() -> bool {
+    if (!__syncthreads_and(mbar_wait(bar, 0) ? 1 : 0)) {
+      if (tid == 0) atomicAdd(&g_fast_wait_failures, 1);
+      return false;
+    }
+    return true;
+  };
+
   float2 v[E];
+  if constexpr (St::kRowTma) {
+    if (!staged()) return;
 #pragma unroll
-  for (int m = 0; m < E; ++m) {
-    if constexpr (M == Mode::kFwdFromX) {
-      v[m] = xl[m * step];
-    } else if constexpr (M == Mode::kBlurMag) {
-      const float2 xv = xl[m * step];
-      v[m] = {sqrtf(xv.x * xv.x + xv.y * xv.y), 0.0f};
-    } else {
-      v[m] = wl[m * step];
+    for (int m = 0; m < E; ++m) v[m] = wtile[l * L + t + T * m];
+    __syncthreads();  // region W becomes the exchange buffer
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      if constexpr (M == Mode::kFwdFromX) {
+        v[m] = xl[m * step];
+      } else if constexpr (M == Mode::kBlurMag) {
+        const float2 xv = xl[m * step];
+        v[m] = {sqrtf(xv.x * xv.x + xv.y * xv.y), 0.0f};
+      } else {
+        v[m] = wl[m * step];
+      }
     }
   }
 
   constexpr bool kStartsInverse = M == Mode::kInv || M == Mode::kUpd;
   transform<L, kStartsInverse>(v, t, tw, row);
 
-  if constexpr (St::kAmp || St::kUpd) {
-    // Every thread waits (bounded); if any gave up, the CTA records it and
-    // leaves together, writing nothing.
-    if (!__syncthreads_and(mbar_wait(bar, 0) ? 1 : 0)) {
-      if (tid == 0) atomicAdd(&g_fast_wait_failures, 1);
-      return;
-    }
+  if constexpr (St::kAmp) {
+    if (!staged()) return;
   }
 
   if constexpr (M == Mode::kMod) {
@@ -292,7 +321,8 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
       cb = p.ctrl->b;
     }
     if constexpr (St::kUpd) {
-      const float2* x_tile = reinterpret_cast<const float2*>(sbase + St::kExchange);
+      // x_new replaces the old iterate in its tile and leaves by one bulk store.
+      float2* x_tile = reinterpret_cast<float2*>(sbase + St::kExchange);
       const std::uint8_t* s_tile = sbase + St::kExchange + St::kSideA;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
@@ -302,8 +332,14 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
           const float2 xo = x_tile[j];
           xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
         }
-        xl[m * step] = xn;
+        x_tile[j] = xn;
         v[m] = xn;
+      }
+      fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        bulk_s2g(p.x + line0 * L, x_tile, St::kTile);
+        bulk_commit();
       }
     } else {
       const std::uint8_t* __restrict__ sl = p.support + base;
@@ -317,9 +353,9 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
         xl[m * step] = xn;
         v[m] = xn;
       }
+      __syncthreads();
     }
     if (p.bump_counter && blockIdx.x == 0 && tid == 0) ++p.ctrl->counters[p.group];
-    __syncthreads();
     transform<L, false>(v, t, tw, row);
   } else if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
     const float inv_l = 1.0f / static_cast<float>(L);
@@ -330,6 +366,21 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
       v[m] = cscale(v[m], expf(p.blur_k * f * f) * inv_l);
     }
     transform<L, true>(v, t, tw, row);
+  }
+
+  if constexpr (St::kRowTma) {
+    // The transform's last stage ran in registers after a barrier, so region W
+    // is free: the output tile goes there and leaves by one bulk store.
+#pragma unroll
+    for (int m = 0; m < E; ++m) wtile[l * L + t + T * m] = v[m];
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      bulk_s2g(p.w + line0 * L, wtile, St::kTile);
+      bulk_commit();
+      bulk_wait_reads();
+    }
+    return;
   }
 
   float peak = 0.0f;

@@ -257,7 +257,13 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   if (!problem.amplitude || !problem.support) {
     throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
   }
-  batch_ = options.variant == Variant::kPlain ? 1 : (options.batch ? options.batch : starts_);
+  if (options.variant == Variant::kPlain) {
+    batch_ = 1;
+  } else if (options.batch) {
+    batch_ = options.batch;
+  } else {
+    batch_ = options.tune ? tuned_batch(problem, options) : starts_;
+  }
   groups_ = starts_ / batch_;
   options_.start = nullptr;
 
@@ -337,7 +343,11 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   stream_.sync();
 }
 
-Solver::~Solver() { cudaStreamSynchronize(stream_); }
+Solver::~Solver() {
+  cudaStreamSynchronize(stream_);
+  graphs_.clear();
+  for (cudaEvent_t e : branch_events_) cudaEventDestroy(e);
+}
 
 PassParams Solver::base(Mode mode, int axis3, int g) const {
   PassParams p = runner_.params(mode, axis3, batch_);
@@ -370,12 +380,12 @@ void Solver::establish_wave() {
 // One iteration of group g (cpu_solver.cpp:84-89): forward FFT, modulus with
 // the error, inverse FFT, update; the x-axis forward of the new iterate is
 // folded into the update pass.
-void Solver::enqueue_iteration(int g) {
+void Solver::enqueue_iteration(int g, cudaStream_t s) {
   const int outer = runner_.outer();
-  runner_.launch(Mode::kMod, outer, base(Mode::kMod, outer, g), stream_);
-  if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, base(Mode::kInv, 1, g), stream_);
-  runner_.launch(Mode::kUpd, 2, base(Mode::kUpd, 2, g), stream_);
-  if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+  runner_.launch(Mode::kMod, outer, base(Mode::kMod, outer, g), s);
+  if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, base(Mode::kInv, 1, g), s);
+  runner_.launch(Mode::kUpd, 2, base(Mode::kUpd, 2, g), s);
+  if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), s);
 }
 
 void Solver::run(const OpDesc* ops, std::size_t count) {
@@ -437,10 +447,29 @@ void Solver::iterate(int count, Coefficients c) {
       trace("iterate chunk len=%d graph=%s", len, it == graphs_.end() ? "capture" : "cached");
       if (it == graphs_.end()) {
         const unsigned long long before = launches();
+        if (groups_ > 1 && branches_.empty()) {
+          // one branch stream per group plus a fork event and a join event per group
+          for (int g = 0; g < groups_; ++g) branches_.push_back(std::make_unique<Stream>());
+          branch_events_.resize(static_cast<std::size_t>(groups_) + 1);
+          for (auto& e : branch_events_) {
+            QPB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+          }
+        }
         QPB_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
-          for (int g = 0; g < groups_; ++g) {
-            for (int i = 0; i < len; ++i) enqueue_iteration(g);
+          if (groups_ > 1) {
+            // Independent start groups become parallel branches of the graph, so
+            // one group's modulus pass can overlap another group's update pass.
+            QPB_CHECK(cudaEventRecord(branch_events_[0], stream_));
+            for (int g = 0; g < groups_; ++g) {
+              cudaStream_t s = *branches_[g];
+              QPB_CHECK(cudaStreamWaitEvent(s, branch_events_[0], 0));
+              for (int i = 0; i < len; ++i) enqueue_iteration(g, s);
+              QPB_CHECK(cudaEventRecord(branch_events_[g + 1], s));
+              QPB_CHECK(cudaStreamWaitEvent(stream_, branch_events_[g + 1], 0));
+            }
+          } else {
+            for (int i = 0; i < len; ++i) enqueue_iteration(0, stream_);
           }
         } catch (...) {
           cudaGraph_t broken{};
@@ -457,7 +486,7 @@ void Solver::iterate(int count, Coefficients c) {
       it->second->launch(stream_);
     } else {
       for (int g = 0; g < groups_; ++g) {
-        for (int i = 0; i < len; ++i) enqueue_iteration(g);
+        for (int i = 0; i < len; ++i) enqueue_iteration(g, stream_);
       }
     }
     done += len;

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "aux_kernels.cuh"
@@ -115,7 +116,17 @@ struct SolverOptions {
   AmpStorage amp_storage = AmpStorage::kF32;
   int device = -1;                  // CUDA ordinal; -1 = the current device
   cudaStream_t stream = nullptr;    // work stream lent by the caller; null = own stream
+  bool tune = true;                 // batch == 0: let the autotuner pick starts per launch
 };
+
+// Starts per launch the autotuner picks for this problem and start count: the
+// fastest of starts, starts/2, starts/4, starts/8 (divisors only), timed once
+// per (device, shape, starts, amplitude storage) on scratch solvers and cached
+// for the process. QPB_TUNE=0 disables it (all starts in one launch).
+int tuned_batch(const ProblemView& problem, const SolverOptions& options);
+
+// The cached choices, for reporting: one line per tuned configuration.
+std::string tuning_report();
 
 // One recipe operation, the POD form of qpcu::Op (recipe.hpp:44).
 enum OpKind : int { kOpER = 0, kOpHIO = 1, kOpRAAR = 2, kOpShrinkwrap = 3, kOpDetwinBegin = 4,
@@ -188,7 +199,7 @@ class Solver {
   }
   PassParams base(Mode mode, int axis3, int g) const;
 
-  void enqueue_iteration(int g);
+  void enqueue_iteration(int g, cudaStream_t s);
   void enqueue_establish(int g);
   void establish_wave();
   void iterate(int count, Coefficients c);
@@ -232,6 +243,9 @@ class Solver {
   int capacity_ = 0;
   bool wave_valid_ = false;
   std::map<int, std::unique_ptr<Graph>> graphs_;
+  // Captured graphs run start groups as parallel branches, one stream each.
+  std::vector<std::unique_ptr<Stream>> branches_;
+  std::vector<cudaEvent_t> branch_events_;
   std::vector<std::vector<float>> errors_;
   std::vector<double> host_errs_;
   int iteration_ = 0;
