@@ -187,6 +187,23 @@ QPB_API qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape,
                                                const float* x, float* out, float* error_out,
                                                void* stream);
 
+/* Amplitude loss and its gradient for gradient-based reconstruction (no
+ * counterpart in the reference, whose solvers only project): for each of
+ * `batch` objects x_b, loss[b] = sum over usable pixels of (|F x_b| - A)^2
+ * with F the unitary FFT, and grad[b] = dL/dRe x_b + i dL/dIm x_b =
+ * 2 F^H[(|y| - A) y / |y|] = 2 (x_b - P_M x_b) with the modulus projection of
+ * qpb_modulus_project (src/cpu/kernels.cpp:25-42 in the reference).
+ *   Device pointers, FFT order (numpy ifftshift of centre-origin arrays):
+ * signed_amplitude (numel floats, the amplitude with -1 on masked pixels),
+ * x and grad (batch * numel complex64, distinct), loss (batch doubles).
+ * Enqueued on `stream` (cudaStream_t; NULL = legacy default stream); returns
+ * without waiting. The first call per device and shape builds line plans
+ * (device allocations kept for the process); calls on one device share a
+ * control block, so calls that overlap on the GPU race. */
+QPB_API qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int batch,
+                                           const float* signed_amplitude, const float* x,
+                                           float* grad, double* loss, void* stream);
+
 /* Single operators on centre-origin arrays (qpcu::cuda::, operators.hpp:25-33). */
 QPB_API qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
                                float* error_out);

@@ -52,6 +52,7 @@ EXPORTS = (
     "qpb_kernel_launches",
     "qpb_tuning_report",
     "qpb_profile_passes",
+    "qpb_amplitude_loss_grad",
     "qpb_modulus_project_noalloc",
     "qpb_modulus_project",
     "qpb_support_project",
@@ -141,6 +142,8 @@ def load():
         lib.qpb_profile_passes.argtypes = [c_void_p, c_int, POINTER(c_double), POINTER(c_int)]
         lib.qpb_tuning_report.argtypes = [c_char_p, c_size_t]
         lib.qpb_modulus_project.argtypes = [POINTER(Problem), c_void_p, c_int, POINTER(c_float)]
+        lib.qpb_amplitude_loss_grad.argtypes = [c_int, POINTER(c_int64), c_int, c_void_p,
+                                                c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_modulus_project_noalloc.argtypes = [c_int, POINTER(c_int64), c_void_p, c_void_p,
                                                     c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_support_project.argtypes = [c_void_p, c_void_p, c_size_t]

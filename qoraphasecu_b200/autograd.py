@@ -1,0 +1,158 @@
+"""Differentiable amplitude loss for gradient-based reconstruction.
+
+``AmplitudeLoss`` is a ``torch.autograd.Function`` whose forward and backward
+run the hand-written loss/adjoint line passes of libqpb.so
+(``qpb_amplitude_loss_grad``): for each object x_b of a batch,
+
+    L_b(x) = sum over usable pixels of (|F x_b| - A)^2,     F the unitary FFT,
+    dL_b/dRe x + i dL_b/dIm x = 2 F^H[(|y| - A) y / |y|] = 2 (x_b - P_M x_b),
+
+P_M being the reference's modulus projection. The gradient is computed in
+the forward call and kept for backward. Objects live in FFT order on the
+device (``to_fft_order`` / ``to_centred`` convert); PyTorch only holds the
+memory and runs the optimiser step.
+
+``adam_reconstruct`` is the gradient-based counterpart of ``reconstruct``:
+random starts drawn exactly as the projection solver draws them, Adam on the
+amplitude loss, and the support projection after every step.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .api import Problem, Reconstruction, Solver
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class AmplitudeModel:
+    """The problem's signed amplitude (-1 on masked pixels) and support, FFT order, on a device."""
+
+    def __init__(self, problem: Problem, device: str = "cuda"):
+        torch = _torch()
+        amp = np.fft.ifftshift(problem.amplitude).astype(np.float32)
+        mask = np.fft.ifftshift(problem.mask)
+        signed = np.where(mask != 0, np.float32(-1.0), amp).astype(np.float32)
+        self.shape = tuple(problem.shape)
+        self.signed = torch.from_numpy(np.ascontiguousarray(signed)).to(device)
+        self.support = torch.from_numpy(
+            np.ascontiguousarray(np.fft.ifftshift(problem.support) != 0)).to(device)
+        self.energy = float(np.sum(np.where(mask != 0, 0.0, amp.astype(np.float64) ** 2)))
+
+
+def _loss_and_grad(x, signed, shape):
+    torch = _torch()
+    if not x.is_cuda or x.dtype != torch.complex64:
+        raise ValueError("x must be a complex64 CUDA tensor")
+    x = x.contiguous()
+    batch = x.numel() // int(np.prod(shape))
+    if batch * int(np.prod(shape)) != x.numel():
+        raise ValueError(f"x of {x.numel()} elements is not a batch of {shape}")
+    grad = torch.empty_like(x)
+    loss = torch.empty(batch, dtype=torch.float64, device=x.device)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    _lib.check(lib.qpb_amplitude_loss_grad(
+        len(shape), _lib.shape_arg(shape), batch, ctypes.c_void_p(signed.data_ptr()),
+        ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
+        ctypes.c_void_p(loss.data_ptr()), ctypes.c_void_p(stream)))
+    return loss, grad
+
+
+class AmplitudeLoss:
+    """``AmplitudeLoss.apply(x, model)`` -> per-object losses (float64, shape (batch,))."""
+
+    _function = None
+
+    @classmethod
+    def function(cls):
+        if cls._function is None:
+            torch = _torch()
+
+            class _Fn(torch.autograd.Function):
+                @staticmethod
+                def forward(ctx, x, signed, shape):
+                    loss, grad = _loss_and_grad(x, signed, shape)
+                    ctx.save_for_backward(grad)
+                    ctx.ndim = len(shape)
+                    return loss
+
+                @staticmethod
+                def backward(ctx, g):
+                    (grad,) = ctx.saved_tensors
+                    scale = g.to(torch.float32).reshape(-1, *([1] * ctx.ndim))
+                    return grad * scale, None, None
+
+            cls._function = _Fn
+        return cls._function
+
+    @classmethod
+    def apply(cls, x, model: AmplitudeModel):
+        batch_shape = x.shape[: x.dim() - len(model.shape)]
+        if tuple(x.shape[x.dim() - len(model.shape):]) != model.shape:
+            raise ValueError(f"x.shape {tuple(x.shape)} does not end with {model.shape}")
+        losses = cls.function().apply(x, model.signed, model.shape)
+        return losses.reshape(batch_shape) if batch_shape else losses.reshape(())
+
+
+def amplitude_loss(x, model: AmplitudeModel):
+    """Per-object amplitude losses of FFT-order objects x (..., *shape)."""
+    return AmplitudeLoss.apply(x, model)
+
+
+def to_fft_order(x, ndim):
+    """Centre-origin -> FFT order over the last ``ndim`` axes (torch tensors)."""
+    torch = _torch()
+    return torch.fft.ifftshift(x, dim=tuple(range(-ndim, 0)))
+
+
+def to_centred(x, ndim):
+    """FFT order -> centre-origin over the last ``ndim`` axes (torch tensors)."""
+    torch = _torch()
+    return torch.fft.fftshift(x, dim=tuple(range(-ndim, 0)))
+
+
+def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr: float = 1e-2,
+                     seed: int | None = None, init=None, seconds: float | None = None,
+                     device: str = "cuda"):
+    """Gradient-based reconstruction: Adam on the amplitude loss with the
+    support projection after every step. Starts are drawn as ``Solver`` draws
+    them (same seed -> same starting objects). Stops after ``steps`` steps or
+    ``seconds`` of wall time, whichever comes first. Returns one
+    ``Reconstruction`` per start; ``errors`` holds the Fourier error
+    sqrt(L / energy) of every step, the projection solvers' error measure."""
+    torch = _torch()
+    with Solver(problem, starts=starts, seed=seed, init=init) as drawn:
+        first = drawn.results()
+    model = AmplitudeModel(problem, device)
+    ndim = len(model.shape)
+    x0 = np.stack([np.fft.ifftshift(r.object) for r in first]).astype(np.complex64)
+    x = torch.from_numpy(x0).to(device).requires_grad_(True)
+    support = model.support.to(torch.complex64)
+    opt = torch.optim.Adam([x], lr=lr)
+    history = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        opt.zero_grad(set_to_none=True)
+        losses = amplitude_loss(x, model)
+        losses.sum().backward()
+        history.append(losses.detach())
+        opt.step()
+        with torch.no_grad():
+            x.mul_(support)
+        if seconds is not None and time.perf_counter() - t0 >= seconds:
+            break
+    torch.cuda.synchronize()
+    errors = torch.sqrt(torch.stack(history) / (model.energy + 1e-12)).to(torch.float32).cpu().numpy()
+    final = to_centred(x.detach(), ndim).cpu().numpy()
+    supp = np.fft.fftshift(model.support.cpu().numpy(), axes=tuple(range(-ndim, 0)))
+    return [Reconstruction(final[s], supp.copy(), errors[:, s].copy()) for s in range(starts)]

@@ -1,0 +1,97 @@
+// The amplitude loss L(x) = sum over usable pixels of (|F x| - A)^2 (F the
+// unitary FFT) and its gradient, for gradient-based reconstruction.
+//
+// The gradient in PyTorch's convention (dL/dRe x + i dL/dIm x) is
+// 2 F^H[(|y| - A) y / |y|], y = F x, which equals 2 (x - P_M x) with the
+// reference's modulus projection P_M (src/cpu/kernels.cpp:25-42) up to its
+// eps. It is computed by the same fused line passes as a modulus projection:
+// forward transform, the gradient's point-wise step with the loss sum on the
+// outer axis, inverse transform.
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../../include/qpb.h"
+#include "solver.hpp"
+
+namespace qpb {
+
+namespace {
+
+// Line plans, a control block and a zero counter per device, created on the
+// first call and kept for the process.
+struct AdjointResources {
+  PlanCache plans;
+  DeviceBuffer<Ctrl> ctrl{1};
+  DeviceBuffer<int> counter{1};
+};
+
+AdjointResources& resources() {
+  static std::mutex mutex;
+  static std::map<int, std::unique_ptr<AdjointResources>> per_device;
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  auto& slot = per_device[device];
+  if (!slot) slot = std::make_unique<AdjointResources>();
+  return *slot;
+}
+
+}  // namespace
+
+void amplitude_loss_grad(int ndim, const long long* shape, int batch, const float* signed_amp,
+                         const float2* x, float2* grad, double* loss, cudaStream_t stream) {
+  if (batch < 1) throw InvalidArgument("batch must be >= 1");
+  ProblemView view;
+  view.ndim = ndim;
+  for (int a = 0; a < ndim && a < 3; ++a) view.shape[a] = shape[a];
+  const Dims3 d = dims_of(view);
+  AdjointResources& r = resources();
+  PassRunner runner(d, ndim, r.plans);
+  QPB_CHECK(cudaMemsetAsync(r.counter.get(), 0, sizeof(int), stream));
+  QPB_CHECK(cudaMemsetAsync(loss, 0, sizeof(double) * batch, stream));
+  set_ctrl(r.ctrl.get(), Ctrl{loss, 1, 0.0f, 0.0f, r.counter.get()}, stream);
+  auto params = [&](Mode m, int axis3) {
+    PassParams p = runner.params(m, axis3, batch);
+    p.w = grad;
+    p.x = const_cast<float2*>(x);
+    p.amp = signed_amp;
+    p.ctrl = r.ctrl.get();
+    p.starts_total = batch;
+    p.amp_storage = AmpStorage::kF32;
+    return p;
+  };
+  const int outer = runner.outer();
+  runner.launch(Mode::kFwdFromX, 2, params(Mode::kFwdFromX, 2), stream);
+  if (runner.has_mid()) runner.launch(Mode::kFwd, 1, params(Mode::kFwd, 1), stream);
+  runner.launch(Mode::kGrad, outer, params(Mode::kGrad, outer), stream);
+  if (runner.has_mid()) runner.launch(Mode::kInv, 1, params(Mode::kInv, 1), stream);
+  runner.launch(Mode::kInv, 2, params(Mode::kInv, 2), stream);
+}
+
+}  // namespace qpb
+
+extern "C" qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int batch,
+                                              const float* signed_amplitude, const float* x,
+                                              float* grad, double* loss, void* stream) {
+  try {
+    qpb::clear_last_error();
+    if (!shape || !signed_amplitude || !x || !grad || !loss) {
+      throw qpb::InvalidArgument("NULL argument");
+    }
+    long long sh[3] = {0, 0, 0};
+    for (int a = 0; a < ndim && a < 3; ++a) sh[a] = shape[a];
+    qpb::amplitude_loss_grad(ndim, sh, batch, signed_amplitude,
+                             reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(grad),
+                             loss, static_cast<cudaStream_t>(stream));
+    return QPB_OK;
+  } catch (const std::invalid_argument& e) {
+    qpb::set_last_error(e.what());
+    return QPB_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    qpb::set_last_error(e.what());
+    return QPB_RUNTIME_ERROR;
+  }
+}

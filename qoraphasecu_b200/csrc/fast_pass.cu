@@ -27,6 +27,7 @@
 #include "bulk_copy.cuh"
 #include "butterfly.cuh"
 #include "fast_pass.cuh"
+#include "projection.cuh"
 #include "reduce.cuh"
 
 namespace qpb {
@@ -153,7 +154,7 @@ struct Staging {
   static constexpr int kTile = G::LINES * L * 8;  // one complex64 tile
   static constexpr bool kRowTma =
       ROWS && (M == Mode::kFwd || M == Mode::kFwdFromX || M == Mode::kInv || M == Mode::kUpd);
-  static constexpr bool kAmp = M == Mode::kMod;
+  static constexpr bool kAmp = M == Mode::kMod || M == Mode::kGrad;
   static constexpr bool kUpd = M == Mode::kUpd && ROWS;
   static constexpr int kExchange = align16(kRowTma && kTile > G::SMEM ? kTile : G::SMEM);
   static constexpr int kSideA =
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
     if (!staged()) return;
   }
 
-  if constexpr (M == Mode::kMod) {
+  if constexpr (M == Mode::kMod || M == Mode::kGrad) {
     const float s = p.scale;
     float acc = 0.0f;
     const AmpT* amp_tile = reinterpret_cast<const AmpT*>(sbase + St::kExchange);
@@ -291,18 +292,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
     for (int m = 0; m < E; ++m) {
       const int j = t + T * m;
       const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * G::LINES + l]);
-      const float re = v[m].x * s;
-      const float im = v[m].y * s;
-      const float mag = sqrtf(re * re + im * im);
-      float target = mag;
-      if (a >= 0.0f) {
-        const float d = mag - a;
-        acc += d * d;
-        target = a;
-      }
-      // approximate division (<= 2 ulp): branch-free, far inside the tolerance
-      const float f = __fdividef(target, mag + kEps) * s;
-      v[m] = {re * f, im * f};
+      v[m] = pointwise_projection<M>(v[m], a, s, acc);
     }
     const double total = block_sum_double(static_cast<double>(acc));
     if (tid == 0) {
@@ -426,7 +416,7 @@ void launch_one(const PassParams& p, cudaStream_t stream) {
 
 template <int L, bool ROWS, Mode M>
 void launch_storage(const PassParams& p, cudaStream_t stream) {
-  if constexpr (M == Mode::kMod) {
+  if constexpr (M == Mode::kMod || M == Mode::kGrad) {
     switch (p.amp_storage) {
       case AmpStorage::kF32:
         return launch_one<L, ROWS, M, float>(p, stream);
@@ -457,6 +447,8 @@ void launch_mode(Mode mode, const PassParams& p, cudaStream_t stream) {
       return launch_storage<L, ROWS, Mode::kBlur>(p, stream);
     case Mode::kBlurMag:
       return launch_storage<L, ROWS, Mode::kBlurMag>(p, stream);
+    case Mode::kGrad:
+      return launch_storage<L, ROWS, Mode::kGrad>(p, stream);
   }
 }
 
@@ -507,6 +499,9 @@ void allow_smem_modes() {
   allow_smem_one<L, ROWS, Mode::kUpd, float>();
   allow_smem_one<L, ROWS, Mode::kBlur, float>();
   allow_smem_one<L, ROWS, Mode::kBlurMag, float>();
+  allow_smem_one<L, ROWS, Mode::kGrad, float>();
+  allow_smem_one<L, ROWS, Mode::kGrad, __half>();
+  allow_smem_one<L, ROWS, Mode::kGrad, __nv_bfloat16>();
 }
 
 template <int L>

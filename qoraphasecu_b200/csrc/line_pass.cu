@@ -18,6 +18,7 @@
 #include "butterfly.cuh"
 #include "fast_pass.cuh"
 #include "line_pass.cuh"
+#include "projection.cuh"
 #include "reduce.cuh"
 
 namespace qpb {
@@ -196,9 +197,9 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(const PassParams p)
   float2* res = run_stages<kStartsInverse>(p, buf_a, buf_b, ldl);
   float2* other = res == buf_a ? buf_b : buf_a;
 
-  if constexpr (M == Mode::kMod) {
-    // P_M on the unnormalised transform: scale by s in, and by s out so that the
-    // unnormalised inverse lands on the unitary result.
+  if constexpr (M == Mode::kMod || M == Mode::kGrad) {
+    // P_M (or the loss gradient) on the unnormalised transform: scaled by s in,
+    // and by s out so that the unnormalised inverse lands on the unitary result.
     float acc = 0.0f;
     const float s = p.scale;
     for (int idx = threadIdx.x; idx < tile; idx += blockDim.x) {
@@ -206,18 +207,7 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(const PassParams p)
       tile_coords(p, idx, l, j);
       const long long e = element(p, line0 + l, j) - start_off;
       const float a = load_amp<AmpT>(p.amp, e);
-      float2 v = res[l * ldl + j];
-      const float re = v.x * s;
-      const float im = v.y * s;
-      const float mag = sqrtf(re * re + im * im);
-      float target = mag;
-      if (a >= 0.0f) {
-        const float d = mag - a;
-        acc += d * d;
-        target = a;
-      }
-      const float f = target / (mag + kEps) * s;
-      res[l * ldl + j] = {re * f, im * f};
+      res[l * ldl + j] = pointwise_projection<M>(res[l * ldl + j], a, s, acc);
     }
     const double total = block_sum_double(static_cast<double>(acc));
     if (threadIdx.x == 0) {
@@ -321,7 +311,7 @@ void launch_mode(const PassParams& p, cudaStream_t stream) {
     QPB_CHECK(cudaGetLastError());
     count_launches(1);
   };
-  if constexpr (M == Mode::kMod) {
+  if constexpr (M == Mode::kMod || M == Mode::kGrad) {
     switch (p.amp_storage) {
       case AmpStorage::kF32:
         launch(line_pass_kernel<M, float>);
@@ -357,6 +347,9 @@ void configure_line_passes() {
   allow_smem(line_pass_kernel<Mode::kUpd, float>);
   allow_smem(line_pass_kernel<Mode::kBlur, float>);
   allow_smem(line_pass_kernel<Mode::kBlurMag, float>);
+  allow_smem(line_pass_kernel<Mode::kGrad, float>);
+  allow_smem(line_pass_kernel<Mode::kGrad, __half>);
+  allow_smem(line_pass_kernel<Mode::kGrad, __nv_bfloat16>);
   configure_fast_passes();
 }
 
@@ -391,6 +384,8 @@ void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
       return launch_mode<Mode::kBlur>(p, stream);
     case Mode::kBlurMag:
       return launch_mode<Mode::kBlurMag>(p, stream);
+    case Mode::kGrad:
+      return launch_mode<Mode::kGrad>(p, stream);
   }
 }
 

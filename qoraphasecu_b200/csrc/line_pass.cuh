@@ -25,7 +25,10 @@ enum class Mode : int {
   kUpd,      // P <- IFFT(w); x <- S ? P : a x + b P; w <- FFT(x)
   kBlur,     // w <- IFFT(g FFT(w)), g = exp(k f^2) / L along this axis
   kBlurMag,  // as kBlur on (|x|, 0)
+  kGrad,     // w <- IFFT(2 (1 - A / (|y| + eps)) y), y = FFT(w), and sum (|y| - A)^2:
+             // the gradient of the amplitude loss, 2 (x - P_M x)
 };
+
 
 enum class AmpStorage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 
