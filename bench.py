@@ -198,17 +198,23 @@ def run_reference(args):
     return 0
 
 
-def run_profile(iterations):
-    """The benchmark workload cut to a few iterations launched directly (no graph),
-    so that an ncu capture sees each line pass of the timed loop after a short
-    set-up: make_problem, solver construction, `iterations` RAAR iterations."""
+def run_profile(iterations, schedule="streamed"):
+    """The benchmark workload cut to a few iterations, all 32 starts in one
+    launch per pass and no autotuning, so that an ncu capture sees each line
+    pass after a short set-up: make_problem, solver construction, `iterations`
+    RAAR iterations."""
     import qoraphasecu_b200 as qpc
     from qoraphasecu_b200 import workloads
     from qoraphasecu_b200.recipe import RAAR, Recipe
 
     _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
     problem = qpc.make_problem(intensity, mask=mask)
-    with qpc.Solver(problem, starts=STARTS, seed=0, variant="batched", sync_every=1) as solver:
+    if schedule == "resident":
+        # one launch runs every iteration
+        kw = dict(schedule="resident", sync_every=iterations)
+    else:
+        kw = dict(schedule="streamed", batch=STARTS, sync_every=1)
+    with qpc.Solver(problem, starts=STARTS, seed=0, variant="batched", **kw) as solver:
         solver.run(Recipe(RAAR(iterations, 0.9)))
         print(json.dumps({"profile_iterations": iterations,
                           "kernels": qpc.kernel_launches(),
@@ -247,11 +253,13 @@ def main(argv=None):
     parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
     parser.add_argument("--profile", type=int, default=0, metavar="ITERS",
                         help="only build the workload and run ITERS RAAR iterations (for ncu)")
+    parser.add_argument("--schedule", choices=("auto", "streamed", "resident"), default="auto",
+                        help="batched schedule of the timed solver (auto = autotuned)")
     parser.add_argument("--profile-step", action="store_true",
                         help="only build the workload and run one benchmark step (for ncu)")
     args = parser.parse_args(argv)
     if args.profile:
-        return run_profile(args.profile)
+        return run_profile(args.profile, "resident" if args.schedule == "resident" else "streamed")
     if args.profile_step:
         return run_profile_step(args.sync_every)
     if args.warmup < 3 and args.impl == "ours":
@@ -296,7 +304,8 @@ def main(argv=None):
     stream = torch.cuda.current_stream()
     problem = qpc.make_problem(intensity, mask=mask)
     solver = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
-                        batch=args.batch or None, device=local, stream=stream.cuda_stream)
+                        batch=args.batch or None, device=local, stream=stream.cuda_stream,
+                        schedule=args.schedule)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):

@@ -44,6 +44,18 @@ typedef enum qpb_amp_storage { QPB_AMP_F32 = 0, QPB_AMP_F16 = 1, QPB_AMP_BF16 = 
  * directly (the in-repo baseline). Replaces qpcu::Variant (solver.hpp:21-29). */
 typedef enum qpb_variant { QPB_VARIANT_BATCHED = 0, QPB_VARIANT_PLAIN = 1 } qpb_variant;
 
+/* How BATCHED iterations run (no counterpart in the reference). STREAMED: two
+ * line passes per 2D iteration (four in 3D) through HBM, start groups as
+ * parallel graph branches. RESIDENT: square 2D problems of side 64, 128 or 256
+ * only; each start's iterate stays in the shared memory of a thread-block
+ * cluster for a whole chunk of sync_every iterations, one launch per chunk.
+ * AUTO: the autotuner times the candidates once per shape and start count. */
+typedef enum qpb_schedule {
+  QPB_SCHEDULE_AUTO = 0,
+  QPB_SCHEDULE_STREAMED = 1,
+  QPB_SCHEDULE_RESIDENT = 2
+} qpb_schedule;
+
 /* A made problem: the fields of qpcu::Problem (problem.hpp:26-31). */
 typedef struct qpb_problem {
   int ndim;                /* 2 or 3 */
@@ -64,6 +76,7 @@ typedef struct qpb_options {
   int amp_storage;         /* qpb_amp_storage */
   int device;              /* CUDA device ordinal; -1 = the calling thread's current device */
   void* stream;            /* cudaStream_t the solver enqueues on; NULL = a stream of its own */
+  int schedule;            /* a qpb_schedule value; used by BATCHED only */
 } qpb_options;
 
 /* One recipe operation: the POD form of qpcu::Op (recipe.hpp:44), the same
@@ -161,7 +174,8 @@ QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
  * between CUDA events on the solver's stream; ms_out[p] receives the mean
  * duration of pass p of one iteration (2D: modulus pass, update pass; 3D adds
  * the y-axis inverse and forward passes) and *n_passes their count (<= 8).
- * Advances the iterate. No counterpart in the reference: it feeds the
+ * With the resident schedule, *n_passes = 1 and ms_out[0] is the mean time per
+ * iteration of one launch running all `iterations`. Advances the iterate. No counterpart in the reference: it feeds the
  * per-kernel roofline that bench.py reports. */
 QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
 

@@ -211,9 +211,12 @@ class Solver:
                  seed: int | None = None, init=None, sync_every: int = 10,
                  variant: Literal["batched", "plain"] = "batched",
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
-                 device: int = -1, stream: int | None = None):
+                 device: int = -1, stream: int | None = None,
+                 schedule: Literal["auto", "streamed", "resident"] = "auto"):
         if variant not in _lib.VARIANTS:
             raise ValueError(f"unknown variant '{variant}' (this backend has 'batched' and 'plain')")
+        if schedule not in _lib.SCHEDULES:
+            raise ValueError(f"unknown schedule '{schedule}' (auto, streamed or resident)")
         if amp_storage not in _lib.AMP_STORAGE:
             raise ValueError(f"unknown amp_storage '{amp_storage}'")
         self.problem = problem
@@ -230,6 +233,7 @@ class Solver:
         options.amp_storage = _lib.AMP_STORAGE[amp_storage]
         options.device = device
         options.stream = stream
+        options.schedule = _lib.SCHEDULES[schedule]
         self._lib = _lib.load()
         handle = ctypes.c_void_p()
         _lib.check(self._lib.qpb_create(ctypes.byref(problem._c()), ctypes.byref(options),
@@ -258,7 +262,9 @@ class Solver:
 
     def profile_passes(self, iterations: int = 20):
         """Mean device time (ms) of each line pass of one iteration, timed with
-        CUDA events around direct launches; advances the iterate."""
+        CUDA events around direct launches; with the resident schedule, one
+        value: the mean time per iteration of one launch of ``iterations``
+        iterations. Advances the iterate."""
         ms = (ctypes.c_double * 8)()
         n = ctypes.c_int()
         _lib.check(self._lib.qpb_profile_passes(self._handle, iterations, ms, ctypes.byref(n)))
@@ -317,6 +323,7 @@ def reconstruct(
     sync_every: int = 10,
     amp_storage: Literal["f32", "f16", "bf16"] = "f32",
     progress=None,
+    schedule: Literal["auto", "streamed", "resident"] = "auto",
 ) -> Reconstruction | Ensemble:
     """Array in, reconstruction out.
 
@@ -337,6 +344,10 @@ def reconstruct(
             ``"plain"`` (one start per launch).
         amp_storage: ``"f32"``, ``"f16"`` or ``"bf16"`` storage of the amplitude.
         progress: ``fn(iteration, errors)`` every ``sync_every`` iterations.
+        schedule: how batched iterations run: ``"streamed"`` line passes,
+            ``"resident"`` (square 2D of side 64, 128 or 256: each start held in
+            a thread-block cluster's shared memory) or ``"auto"`` (timed once
+            per shape and start count).
     """
     intensity = np.ascontiguousarray(intensity, dtype=np.float32)
     if intensity.ndim not in (2, 3):
@@ -356,7 +367,8 @@ def reconstruct(
         recipe = default_recipe()
     problem = make_problem(intensity, support, mask, support_threshold)
     with Solver(problem, starts=starts, batch=batch, seed=seed, init=init, sync_every=sync_every,
-                variant=variant, amp_storage=amp_storage, progress=progress) as solver:
+                variant=variant, amp_storage=amp_storage, progress=progress,
+                schedule=schedule) as solver:
         solver.run(recipe)
         runs = solver.results()
     return runs[0] if starts == 1 else Ensemble(tuple(runs))

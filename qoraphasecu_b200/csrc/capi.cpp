@@ -188,6 +188,9 @@ qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qp
     if (options->variant != QPB_VARIANT_BATCHED && options->variant != QPB_VARIANT_PLAIN) {
       throw qpb::InvalidArgument("unknown variant");
     }
+    if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_RESIDENT) {
+      throw qpb::InvalidArgument("unknown schedule");
+    }
     const qpb::ProblemView v = view(problem);
     qpb::dims_of(v);
     if (!v.amplitude || !v.support) {
@@ -203,6 +206,7 @@ qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qp
     o.amp_storage = storage_of(options->amp_storage);
     o.device = options->device;
     o.stream = static_cast<cudaStream_t>(options->stream);
+    o.schedule = static_cast<qpb::Schedule>(options->schedule);
     if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
     qpb::trace("qpb_create: starts=%d batch=%d variant=%d shape=%lld,%lld,%lld", o.starts, o.batch,
                options->variant, v.shape[0], v.shape[1], v.shape[2]);

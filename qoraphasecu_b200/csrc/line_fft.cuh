@@ -1,0 +1,116 @@
+// Register-resident Stockham transforms of lines of length L = 16..1024 (powers
+// of two), shared by the streamed line passes and the resident iteration kernel.
+//
+// A line is held by T = L / E threads, E complex values each, in the
+// "stride-T" distribution: thread t owns elements t + T m, m < E. Every stage
+// of radix R (<= E) is E / R butterflies per thread on registers; between
+// stages the values go once through a shared-memory row (written at their
+// Stockham output positions, read back in the stride-T distribution). The last
+// stage's outputs already sit in the stride-T distribution, so a 256-point
+// transform (16 x 16) costs one shared-memory round trip and an inverse
+// transform can start from the forward's registers. Rows are padded (one slot
+// per 16, pitch = 1 mod 16) so that the Stockham writes and the stride-T reads
+// are free of bank conflicts.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "butterfly.cuh"
+#include "common.cuh"
+
+namespace qpb {
+
+__host__ __device__ constexpr int swz(int i) { return i + (i >> 4); }
+
+template <int L>
+struct Geometry {
+  static constexpr int E = L == 32 || L == 64 ? 8 : 16;
+  static constexpr int T = L / E;
+  static constexpr int LINES = T <= 16 ? 256 / T : (L >= 1024 ? 8 : 16);
+  static constexpr int NT = T * LINES;
+  // CTAs per SM the register budget is sized for (registers <= 64K / (NT * MIN_CTAS)).
+  static constexpr int MIN_CTAS = NT <= 256 ? 3 : 1;
+  // Radix of each stage (product = L, each <= E).
+  static constexpr int R0 = L <= 16 ? L : E;
+  static constexpr int R1 = L <= 16 ? 1 : (L / R0 <= E ? L / R0 : E);
+  static constexpr int R2 = L / (R0 * R1);
+  static constexpr int STAGES = L <= 16 ? 1 : (R2 == 1 ? 2 : 3);
+  static constexpr int PITCH = swz(L) + 1;
+  static constexpr int SMEM = STAGES > 1 ? LINES * PITCH * 8 : 0;
+  static_assert(R0 * R1 * R2 == L, "bad factorisation");
+  static_assert(R2 <= E && R1 <= E, "radix above the register count");
+};
+
+template <int R, bool INV>
+__device__ __forceinline__ void butterfly(float2* u) {
+  if constexpr (R == 2) {
+    bfly2<INV>(u[0], u[1]);
+  } else if constexpr (R == 4) {
+    bfly4<INV>(u[0], u[1], u[2], u[3]);
+  } else if constexpr (R == 8) {
+    bfly8<INV>(u);
+  } else if constexpr (R == 16) {
+    bfly16<INV>(u);
+  }
+}
+
+// One Stockham stage of radix R over the thread's E registers. NS is the
+// product of the radices before it; LAST stages leave values in place,
+// others exchange through the line's shared-memory row.
+template <int L, int R, int NS, bool LAST, bool INV>
+__device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
+                                      const float2* __restrict__ tw, float2* row) {
+  using G = Geometry<L>;
+  constexpr int E = G::E;
+  constexpr int T = G::T;
+  constexpr int Q = E / R;
+  constexpr int STEP = L / (NS * R);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    float2 u[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
+    const int j = t + T * q;
+    const int k = j & (NS - 1);
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = __ldg(tw + r * k * STEP);
+        u[r] = INV ? cmulc(u[r], w) : cmul(u[r], w);
+      }
+    }
+    butterfly<R, INV>(u);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q + r * Q] = u[r];
+    } else {
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[swz(base + r * NS)] = u[r];
+    }
+  }
+  if constexpr (!LAST) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = row[swz(t + T * m)];
+    __syncthreads();
+  }
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
+                                          const float2* __restrict__ tw, float2* row) {
+  using G = Geometry<L>;
+  if constexpr (G::STAGES == 1) {
+    stage<L, G::R0, 1, true, INV>(v, t, tw, row);
+  } else if constexpr (G::STAGES == 2) {
+    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
+    stage<L, G::R1, G::R0, true, INV>(v, t, tw, row);
+  } else {
+    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
+    stage<L, G::R1, G::R0, false, INV>(v, t, tw, row);
+    stage<L, G::R2, G::R0 * G::R1, true, INV>(v, t, tw, row);
+  }
+}
+
+}  // namespace qpb

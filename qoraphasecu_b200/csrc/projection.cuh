@@ -1,10 +1,27 @@
 // Device point-wise step shared by the modulus and loss-gradient line passes.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
 #include "common.cuh"
 #include "line_pass.cuh"
 
 namespace qpb {
+
+// An amplitude in its storage type (float, __half or __nv_bfloat16) as float.
+template <class AmpT>
+__device__ __forceinline__ float to_float(AmpT a) {
+  if constexpr (std::is_same_v<AmpT, float>) {
+    return a;
+  } else if constexpr (std::is_same_v<AmpT, __half>) {
+    return __half2float(a);
+  } else {
+    return __bfloat162float(a);
+  }
+}
 
 // The point-wise step of a modulus (kMod) or amplitude-loss gradient (kGrad)
 // pass on one element of the unnormalised forward transform. `s` = 1/sqrt(n)
@@ -19,14 +36,19 @@ template <Mode M>
 __device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float s, float& acc) {
   const float re = v.x * s;
   const float im = v.y * s;
-  const float mag = sqrtf(re * re + im * im);
+  const float ss = re * re + im * im;
+  // 1 / sqrt(|y|^2 + eps^2) stands for 1 / (|y| + eps): equal in FP32 unless
+  // |y| is within a few orders of magnitude of eps = 1e-12, and 0 -> 0 like the
+  // reference. rsqrtf is the hardware approximation (<= 2 ulp), branch-free.
+  const float rinv = rsqrtf(ss + kEps * kEps);
+  const float mag = ss * rinv;
   float f;
   if constexpr (M == Mode::kGrad) {
     f = 0.0f;
     if (a >= 0.0f) {
       const float d = mag - a;
       acc += d * d;
-      f = 2.0f * (1.0f - __fdividef(a, mag + kEps)) * s;
+      f = 2.0f * (1.0f - a * rinv) * s;
     }
   } else {
     float target = mag;
@@ -35,8 +57,7 @@ __device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float 
       acc += d * d;
       target = a;
     }
-    // approximate division (<= 2 ulp): branch-free, far inside the tolerances
-    f = __fdividef(target, mag + kEps) * s;
+    f = target * rinv * s;
   }
   return {re * f, im * f};
 }

@@ -15,6 +15,7 @@
 #include <string>
 
 #include "fast_pass.cuh"
+#include "resident.cuh"
 #include "solver.hpp"
 
 namespace qpb {
@@ -257,14 +258,33 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   if (!problem.amplitude || !problem.support) {
     throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
   }
+  const bool resident_ok = resident_supports(problem.ndim, d_.d1, d_.d2);
+  if (options.schedule == Schedule::kResident) {
+    if (options.variant == Variant::kPlain) {
+      throw InvalidArgument("the resident schedule runs batched starts only");
+    }
+    if (!resident_ok) {
+      throw InvalidArgument("the resident schedule needs a square 2D problem of side 64, 128 or 256");
+    }
+  }
   if (options.variant == Variant::kPlain) {
     batch_ = 1;
+  } else if (options.schedule == Schedule::kResident) {
+    resident_ = true;
   } else if (options.batch) {
     batch_ = options.batch;
+  } else if (options.tune) {
+    SolverOptions o = options;
+    if (!resident_ok) o.schedule = Schedule::kStreamed;
+    const TunedSchedule t = tuned_schedule(problem, o);
+    batch_ = t.batch;
+    resident_ = t.resident;
   } else {
-    batch_ = options.tune ? tuned_batch(problem, options) : starts_;
+    batch_ = starts_;
   }
+  if (resident_) batch_ = starts_;
   groups_ = starts_ / batch_;
+  if (resident_) configure_resident();
   options_.start = nullptr;
 
   const auto amp = host_roll(problem.amplitude, d_, true);
@@ -283,7 +303,7 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
     auto bytes = signed_amplitude(amp, mask, options.amp_storage);
     const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
     const int lines = fast_pass_lines(mod);
-    if (lines > 0 && mod.S > 1) {
+    if (lines > 0 && mod.S > 1 && !resident_) {
       const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
       bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
       amp_tiled_ = true;
@@ -388,6 +408,23 @@ void Solver::enqueue_iteration(int g, cudaStream_t s) {
   if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), s);
 }
 
+void Solver::enqueue_chunk(int len, cudaStream_t s) {
+  ResidentParams p{};
+  p.x = x_.get();
+  p.w = w_.get();
+  p.amp = amp_.get();
+  p.support = support_.get();
+  p.ctrl = ctrl_.get();
+  p.twiddle = runner_.params(Mode::kFwd, 2, starts_).twiddle;
+  p.group = 0;
+  p.start0 = 0;
+  p.starts_total = starts_;
+  p.iterations = len;
+  p.scale = 1.0f / static_cast<float>(d_.d2);
+  p.amp_storage = options_.amp_storage;
+  launch_resident(p, d_.d2, starts_, s);
+}
+
 void Solver::run(const OpDesc* ops, std::size_t count) {
   validate_recipe(ops, count);
   for (std::size_t i = 0; i < count; ++i) {
@@ -468,6 +505,8 @@ void Solver::iterate(int count, Coefficients c) {
               QPB_CHECK(cudaEventRecord(branch_events_[g + 1], s));
               QPB_CHECK(cudaStreamWaitEvent(stream_, branch_events_[g + 1], 0));
             }
+          } else if (resident_) {
+            enqueue_chunk(len, stream_);
           } else {
             for (int i = 0; i < len; ++i) enqueue_iteration(0, stream_);
           }
@@ -499,6 +538,22 @@ void Solver::iterate(int count, Coefficients c) {
 int Solver::profile_passes(int iterations, double* ms) {
   if (iterations < 1) throw InvalidArgument("iterations must be >= 1");
   if (!wave_valid_) establish_wave();
+  if (resident_) {
+    // One launch of `iterations` iterations between two events.
+    cudaEvent_t e0{}, e1{};
+    QPB_CHECK(cudaEventCreate(&e0));
+    QPB_CHECK(cudaEventCreate(&e1));
+    QPB_CHECK(cudaEventRecord(e0, stream_));
+    enqueue_chunk(iterations, stream_);
+    QPB_CHECK(cudaEventRecord(e1, stream_));
+    stream_.sync();
+    float t = 0.0f;
+    QPB_CHECK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ms[0] = static_cast<double>(t) / iterations;
+    return 1;
+  }
   const int outer = runner_.outer();
   struct PassRef {
     Mode mode;

@@ -106,6 +106,13 @@ enum class Variant : int {
   kPlain = 1,    // one start per launch, launched directly: the in-repo baseline
 };
 
+// How batched iterations run.
+enum class Schedule : int {
+  kAuto = 0,      // the autotuner picks (streamed groups or resident)
+  kStreamed = 1,  // two (3D: four) streamed line passes per iteration, start groups as branches
+  kResident = 2,  // one resident-cluster launch per chunk of iterations (square 2D, side 64/128/256)
+};
+
 struct SolverOptions {
   int starts = 1;
   int batch = 0;  // starts per launch; 0 = all (kBatched only)
@@ -117,13 +124,19 @@ struct SolverOptions {
   int device = -1;                  // CUDA ordinal; -1 = the current device
   cudaStream_t stream = nullptr;    // work stream lent by the caller; null = own stream
   bool tune = true;                 // batch == 0: let the autotuner pick starts per launch
+  Schedule schedule = Schedule::kAuto;
 };
 
-// Starts per launch the autotuner picks for this problem and start count: the
-// fastest of starts, starts/2, starts/4, starts/8 (divisors only), timed once
-// per (device, shape, starts, amplitude storage) on scratch solvers and cached
-// for the process. QPB_TUNE=0 disables it (all starts in one launch).
-int tuned_batch(const ProblemView& problem, const SolverOptions& options);
+// The schedule the autotuner picks for this problem and start count: the
+// resident kernel (where it exists) or streamed passes with starts, starts/2,
+// starts/4 or starts/8 starts per launch (divisors only), timed once per
+// (device, shape, starts, amplitude storage) on scratch solvers and cached for
+// the process. QPB_TUNE=0 disables it (streamed, all starts in one launch).
+struct TunedSchedule {
+  int batch;
+  bool resident;
+};
+TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& options);
 
 // The cached choices, for reporting: one line per tuned configuration.
 std::string tuning_report();
@@ -178,6 +191,8 @@ class Solver {
   void run(const OpDesc* ops, std::size_t count);
   std::size_t error_count() const { return errors_.empty() ? 0 : errors_[0].size(); }
   int starts() const { return starts_; }
+  bool resident() const { return resident_; }
+  int batch() const { return batch_; }
   long long numel() const { return n_; }
   int device() const { return select_.device; }
   // objects: starts * numel complex64; supports: starts * numel; errors: starts * error_count().
@@ -200,6 +215,7 @@ class Solver {
   PassParams base(Mode mode, int axis3, int g) const;
 
   void enqueue_iteration(int g, cudaStream_t s);
+  void enqueue_chunk(int len, cudaStream_t s);  // resident: `len` iterations in one launch
   void enqueue_establish(int g);
   void establish_wave();
   void iterate(int count, Coefficients c);
@@ -231,6 +247,7 @@ class Solver {
   double energy_ = 0.0;
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
   bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
+  bool resident_ = false;            // iterations run by the resident kernel
   DeviceBuffer<float2> x_;
   DeviceBuffer<float2> w_;
   DeviceBuffer<std::uint8_t> support_;

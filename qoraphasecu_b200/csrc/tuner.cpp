@@ -1,32 +1,40 @@
-// Autotuner for the batched schedule: how many starts share one launch.
+// Autotuner for the batched schedule: the resident kernel, or streamed passes
+// with how many starts per launch.
 //
-// Starts are independent, so any grouping gives the same iterates; what
-// changes is how the work fills the GPU. One group of all starts is a single
-// chain of kernels per iteration whose last CTAs run with the SMs half idle;
-// several smaller groups become parallel branches of the captured graph, and
-// one group's modulus pass then overlaps another's update pass. The best
-// split depends on the shape, the start count and the device, so it is
-// measured: each candidate runs a short RAAR stage on a scratch solver built
-// from the same problem, and the fastest is cached for the process.
+// Starts are independent, so any schedule gives the same iterates; what
+// changes is how the work fills the GPU. The resident kernel keeps each start
+// in a cluster's shared memory for a whole chunk of iterations, but one start
+// takes up to 8 SMs, so few starts leave SMs idle. With streamed passes, one
+// group of all starts is a single chain of kernels per iteration whose last
+// CTAs run with the SMs half idle; several smaller groups become parallel
+// branches of the captured graph, and one group's modulus pass then overlaps
+// another's update pass. The best choice depends on the shape, the start count
+// and the device, so it is measured: each candidate runs a short RAAR stage on
+// a scratch solver built from the same problem, and the fastest is cached for
+// the process.
 
 #include <chrono>
 #include <cstdlib>
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <string>
 #include <tuple>
 #include <vector>
 
+#include "resident.cuh"
 #include "solver.hpp"
 
 namespace qpb {
 
 namespace {
 
-using Key = std::tuple<int, int, int, int, int, int>;  // device, d0, d1, d2, starts, storage
+// device, d0, d1, d2, starts, storage, resident kernel among the candidates
+using Key = std::tuple<int, int, int, int, int, int, bool>;
 
 std::mutex g_mutex;
-std::map<Key, int> g_choice;
+std::map<Key, TunedSchedule> g_choice;
+// Timings per candidate: batch (starts per launch) or 0 for the resident kernel.
 std::map<Key, std::vector<std::pair<int, double>>> g_timings;
 
 bool tuning_enabled() {
@@ -37,6 +45,7 @@ bool tuning_enabled() {
 double time_candidate(const ProblemView& problem, const SolverOptions& base, int batch) {
   SolverOptions o = base;
   o.batch = batch;
+  o.schedule = batch == 0 ? Schedule::kResident : Schedule::kStreamed;
   o.tune = false;
   o.start = nullptr;
   o.seed = 0;
@@ -58,33 +67,37 @@ double time_candidate(const ProblemView& problem, const SolverOptions& base, int
 
 }  // namespace
 
-int tuned_batch(const ProblemView& problem, const SolverOptions& options) {
+TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& options) {
   const int starts = options.starts;
-  if (starts < 2 || !tuning_enabled()) return starts;
+  const bool resident_ok = options.schedule != Schedule::kStreamed;
+  if (!tuning_enabled() || (starts < 2 && !resident_ok)) return {starts, false};
   const Dims3 d = dims_of(problem);
   int device = 0;
   QPB_CHECK(cudaGetDevice(&device));
-  const Key key{device, d.d0, d.d1, d.d2, starts, static_cast<int>(options.amp_storage)};
+  const Key key{device, d.d0, d.d1, d.d2, starts, static_cast<int>(options.amp_storage),
+                resident_ok};
   std::lock_guard<std::mutex> lock(g_mutex);
   if (auto it = g_choice.find(key); it != g_choice.end()) return it->second;
   std::vector<int> candidates;
+  if (resident_ok) candidates.push_back(0);
   for (int parts : {1, 2, 4, 8}) {
-    if (starts % parts == 0 && (parts == 1 || starts / parts >= 1)) candidates.push_back(starts / parts);
+    if (starts % parts == 0 && starts / parts >= 1) candidates.push_back(starts / parts);
   }
-  int best = starts;
+  TunedSchedule best{starts, false};
   double best_time = 1e30;
   std::vector<std::pair<int, double>> timings;
   for (int batch : candidates) {
     const double t = time_candidate(problem, options, batch);
     timings.emplace_back(batch, t);
-    if (t < best_time * 0.98) {  // prefer fewer groups unless clearly faster
+    if (t < best_time * 0.98) {  // prefer earlier candidates unless clearly slower
       best_time = t;
-      best = batch;
+      best = batch == 0 ? TunedSchedule{starts, true} : TunedSchedule{batch, false};
     }
   }
   g_choice[key] = best;
   g_timings[key] = timings;
-  trace("tuned batch for %dx%dx%d, %d starts: %d", d.d0, d.d1, d.d2, starts, best);
+  trace("tuned schedule for %dx%dx%d, %d starts: %s batch %d", d.d0, d.d1, d.d2, starts,
+        best.resident ? "resident" : "streamed", best.batch);
   return best;
 }
 
@@ -92,12 +105,19 @@ std::string tuning_report() {
   std::lock_guard<std::mutex> lock(g_mutex);
   std::ostringstream out;
   for (const auto& [key, choice] : g_choice) {
-    const auto& [device, d0, d1, d2, starts, storage] = key;
+    const auto& [device, d0, d1, d2, starts, storage, resident_ok] = key;
     out << "device " << device << " shape " << d0 << "x" << d1 << "x" << d2 << " starts "
-        << starts << " storage " << storage << ": batch " << choice << " (";
+        << starts << " storage " << storage << ": "
+        << (choice.resident ? std::string("resident") : "batch " + std::to_string(choice.batch))
+        << " (";
     bool first = true;
     for (const auto& [batch, t] : g_timings[key]) {
-      out << (first ? "" : ", ") << batch << ": " << t * 1e3 << " ms";
+      if (batch == 0) {
+        out << (first ? "" : ", ") << "resident (" << resident_max_clusters(d2) << " clusters of "
+            << resident_cluster(d2) << " CTAs at once): " << t * 1e3 << " ms";
+      } else {
+        out << (first ? "" : ", ") << batch << ": " << t * 1e3 << " ms";
+      }
       first = false;
     }
     out << ")\n";
