@@ -141,6 +141,19 @@ QPB_API qpb_status qpb_half_support(const uint8_t* support, int ndim, const int6
  * the starts. */
 QPB_API qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out);
 
+/* Many problems, any mix of shapes, reconstructed together (no counterpart in
+ * the reference, which builds one solver per problem). options->starts starts
+ * per problem; options->start, when given, holds every problem's starts in
+ * problem order. Problems of one shape share one batched solver (its schedule
+ * autotuned for that shape and start count); every chunk of sync_every
+ * iterations of every shape runs as ONE CUDA graph with the shapes as
+ * parallel branches. qpb_run, qpb_results (problem order: problem q's block of
+ * starts * numel(q) objects and supports, starts * error_count errors, blocks
+ * back to back), qpb_starts (problems * starts) and qpb_destroy work on it;
+ * qpb_profile_passes needs one shape. */
+QPB_API qpb_status qpb_create_batch(const qpb_problem* problems, size_t n_problems,
+                                    const qpb_options* options, qpb_solver** out);
+
 /* qpcu::Solver::run (solver.hpp:72): validates and runs the recipe, continuing
  * from the current state; appends one error per iteration to every start. */
 QPB_API qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);

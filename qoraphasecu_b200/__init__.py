@@ -12,6 +12,7 @@ All public arrays are centre-origin, ``mask=True`` marks an unusable pixel and
 """
 
 from .api import (
+    BatchSolver,
     Ensemble,
     Problem,
     Reconstruction,
@@ -23,12 +24,14 @@ from .api import (
     kernel_launches,
     make_problem,
     reconstruct,
+    reconstruct_batch,
     set_device,
 )
 from .operators import gaussian_blur, modulus_project, support_project
 from .recipe import ER, HIO, RAAR, Recipe, Shrinkwrap, default_recipe, detwin, repeat
 
 __all__ = [
+    "BatchSolver",
     "ER",
     "HIO",
     "RAAR",
@@ -48,6 +51,7 @@ __all__ = [
     "make_problem",
     "modulus_project",
     "reconstruct",
+    "reconstruct_batch",
     "repeat",
     "support_project",
 ]

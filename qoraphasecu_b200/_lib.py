@@ -44,6 +44,7 @@ EXPORTS = (
     "qpb_autocorrelation_support",
     "qpb_half_support",
     "qpb_create",
+    "qpb_create_batch",
     "qpb_run",
     "qpb_set_progress",
     "qpb_error_count",
@@ -132,6 +133,8 @@ def load():
                                                     c_void_p]
         lib.qpb_half_support.argtypes = [c_void_p, c_int, POINTER(c_int64), c_int, c_void_p]
         lib.qpb_create.argtypes = [POINTER(Problem), POINTER(Options), POINTER(c_void_p)]
+        lib.qpb_create_batch.argtypes = [POINTER(Problem), c_size_t, POINTER(Options),
+                                         POINTER(c_void_p)]
         lib.qpb_run.argtypes = [c_void_p, POINTER(Op), c_size_t]
         lib.qpb_set_progress.argtypes = [c_void_p, PROGRESS, c_void_p]
         lib.qpb_error_count.argtypes = [c_void_p, POINTER(c_size_t)]

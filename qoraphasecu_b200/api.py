@@ -203,6 +203,29 @@ def _ops(recipe):
     return array, len(ops)
 
 
+def _options(starts, batch, seed, start, sync_every, variant, amp_storage, device, stream,
+             schedule):
+    if variant not in _lib.VARIANTS:
+        raise ValueError(f"unknown variant '{variant}' (this backend has 'batched' and 'plain')")
+    if schedule not in _lib.SCHEDULES:
+        raise ValueError(f"unknown schedule '{schedule}' (auto, streamed or resident)")
+    if amp_storage not in _lib.AMP_STORAGE:
+        raise ValueError(f"unknown amp_storage '{amp_storage}'")
+    options = _lib.Options()
+    options.starts = starts
+    options.batch = 0 if batch is None else batch
+    options.seed = 0 if seed is None else seed
+    options.start = (start.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+                     if start is not None else None)
+    options.sync_every = sync_every
+    options.variant = _lib.VARIANTS[variant]
+    options.amp_storage = _lib.AMP_STORAGE[amp_storage]
+    options.device = device
+    options.stream = stream
+    options.schedule = _lib.SCHEDULES[schedule]
+    return options
+
+
 class Solver:
     """A live reconstruction: starts drawn on construction; ``run`` continues
     from the current state and appends errors (include/qoraphasecu/solver.hpp:67-74)."""
@@ -213,27 +236,11 @@ class Solver:
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
                  device: int = -1, stream: int | None = None,
                  schedule: Literal["auto", "streamed", "resident"] = "auto"):
-        if variant not in _lib.VARIANTS:
-            raise ValueError(f"unknown variant '{variant}' (this backend has 'batched' and 'plain')")
-        if schedule not in _lib.SCHEDULES:
-            raise ValueError(f"unknown schedule '{schedule}' (auto, streamed or resident)")
-        if amp_storage not in _lib.AMP_STORAGE:
-            raise ValueError(f"unknown amp_storage '{amp_storage}'")
         self.problem = problem
         self.shape = problem.shape
         start = _start(init, problem.shape, starts)
-        options = _lib.Options()
-        options.starts = starts
-        options.batch = 0 if batch is None else batch
-        options.seed = 0 if seed is None else seed
-        options.start = (start.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-                         if start is not None else None)
-        options.sync_every = sync_every
-        options.variant = _lib.VARIANTS[variant]
-        options.amp_storage = _lib.AMP_STORAGE[amp_storage]
-        options.device = device
-        options.stream = stream
-        options.schedule = _lib.SCHEDULES[schedule]
+        options = _options(starts, batch, seed, start, sync_every, variant, amp_storage, device,
+                           stream, schedule)
         self._lib = _lib.load()
         handle = ctypes.c_void_p()
         _lib.check(self._lib.qpb_create(ctypes.byref(problem._c()), ctypes.byref(options),
@@ -307,6 +314,126 @@ class Solver:
         self.close()
 
 
+class BatchSolver:
+    """Many problems, any mix of shapes, reconstructed together.
+
+    Problems of one shape share one batched solver (its schedule autotuned for
+    that shape and start count); every chunk of ``sync_every`` iterations of
+    every shape runs as one CUDA graph with the shapes as parallel branches.
+    ``starts`` starts per problem; ``init``, when given, is one start array per
+    problem (shape ``shape`` or ``(starts, *shape)``). ``results()`` returns
+    one list of reconstructions per problem."""
+
+    def __init__(self, problems, *, starts: int = 1, batch: int | None = None,
+                 seed: int | None = None, init=None, sync_every: int = 10,
+                 variant: Literal["batched", "plain"] = "batched",
+                 amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
+                 device: int = -1, stream: int | None = None,
+                 schedule: Literal["auto", "streamed", "resident"] = "auto"):
+        self.problems = list(problems)
+        if not self.problems:
+            raise ValueError("no problems")
+        start = None
+        if init is not None:
+            if len(init) != len(self.problems):
+                raise ValueError(f"init has {len(init)} entries for {len(self.problems)} problems")
+            start = np.concatenate([_start(i, p.shape, starts).ravel()
+                                    for i, p in zip(init, self.problems)])
+        options = _options(starts, batch, seed, start, sync_every, variant, amp_storage, device,
+                           stream, schedule)
+        self._starts = starts
+        self._views = (_lib.Problem * len(self.problems))(*[p._c() for p in self.problems])
+        self._lib = _lib.load()
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.qpb_create_batch(self._views, len(self.problems),
+                                              ctypes.byref(options), ctypes.byref(handle)))
+        self._handle = handle
+        self._progress = None
+        if progress is not None:
+            self.set_progress(progress)
+
+    def set_progress(self, fn):
+        """``fn(iteration, errors)`` every ``sync_every`` iterations; ``errors``
+        holds problems * starts values, problem by problem."""
+        if fn is None:
+            self._progress = None
+            _lib.check(self._lib.qpb_set_progress(self._handle, _lib.PROGRESS(), None))
+            return
+
+        def trampoline(_user, iteration, errors, count):
+            fn(iteration, np.ctypeslib.as_array(errors, shape=(count,)).copy())
+
+        self._progress = _lib.PROGRESS(trampoline)
+        _lib.check(self._lib.qpb_set_progress(self._handle, self._progress, None))
+
+    def run(self, recipe=None):
+        ops, count = _ops(default_recipe() if recipe is None else recipe)
+        _lib.check(self._lib.qpb_run(self._handle, ops, count))
+
+    def error_count(self) -> int:
+        n = ctypes.c_size_t()
+        _lib.check(self._lib.qpb_error_count(self._handle, ctypes.byref(n)))
+        return n.value
+
+    def profile_passes(self, iterations: int = 20):
+        """As ``Solver.profile_passes``; the problems must share one shape."""
+        ms = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        _lib.check(self._lib.qpb_profile_passes(self._handle, iterations, ms, ctypes.byref(n)))
+        return [ms[i] for i in range(n.value)]
+
+    def results(self):
+        count = self.error_count()
+        sizes = [int(np.prod(p.shape)) for p in self.problems]
+        total = self._starts * sum(sizes)
+        objects = np.empty(total, np.complex64)
+        supports = np.empty(total, np.uint8)
+        errors = np.empty((len(self.problems), self._starts, count), np.float32)
+        _lib.check(self._lib.qpb_results(self._handle, _lib.ptr(objects), _lib.ptr(supports),
+                                         _lib.ptr(errors)))
+        out, at = [], 0
+        for q, p in enumerate(self.problems):
+            block = self._starts * sizes[q]
+            obj = objects[at:at + block].reshape(self._starts, *p.shape)
+            sup = supports[at:at + block].reshape(self._starts, *p.shape).astype(bool)
+            out.append([Reconstruction(obj[s], sup[s], errors[q, s]) for s in range(self._starts)])
+            at += block
+        return out
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.qpb_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def reconstruct_batch(intensities, *, supports=None, masks=None, recipe=None, starts: int = 1,
+                      support_threshold: float = 0.1, **options):
+    """``reconstruct`` over many intensities of any mix of shapes in one batch
+    (:class:`BatchSolver`); returns one Reconstruction (starts == 1) or
+    Ensemble per intensity, in order. ``supports`` / ``masks``: None or one
+    entry (possibly None) per intensity."""
+    intensities = list(intensities)
+    supports = [None] * len(intensities) if supports is None else list(supports)
+    masks = [None] * len(intensities) if masks is None else list(masks)
+    if not (len(supports) == len(masks) == len(intensities)):
+        raise ValueError("supports and masks need one entry per intensity")
+    problems = [make_problem(i, s, m, support_threshold)
+                for i, s, m in zip(intensities, supports, masks)]
+    with BatchSolver(problems, starts=starts, **options) as solver:
+        solver.run(default_recipe() if recipe is None else recipe)
+        runs = solver.results()
+    return [r[0] if starts == 1 else Ensemble(tuple(r)) for r in runs]
+
+
 def reconstruct(
     intensity,
     *,
@@ -375,6 +502,7 @@ def reconstruct(
 
 
 __all__ = [
+    "BatchSolver",
     "Ensemble",
     "Problem",
     "Recipe",
@@ -386,4 +514,5 @@ __all__ = [
     "half_support",
     "make_problem",
     "reconstruct",
+    "reconstruct_batch",
 ]

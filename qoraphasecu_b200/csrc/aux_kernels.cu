@@ -1,5 +1,7 @@
 #include <algorithm>
 
+#include <stdexcept>
+
 #include "aux_kernels.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
@@ -20,10 +22,14 @@ int blocks_for(long long work) {
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; \
        i < (work); i += static_cast<long long>(gridDim.x) * blockDim.x)
 
-__global__ void random_wave_kernel(float2* w, const float* amp, long long n, std::uint64_t seed,
+__global__ void random_wave_kernel(float2* w, const float* amp, long long amp_stride,
+                                   int starts_per_problem, long long n, std::uint64_t seed,
                                    std::uint64_t first_start) {
   const float s = rsqrtf(static_cast<float>(n));
-  const std::uint64_t start = first_start + blockIdx.y;
+  const std::uint64_t global = first_start + blockIdx.y;
+  // Each problem's starts are keyed 0, 1, ... as if it ran alone.
+  const std::uint64_t start = global % static_cast<std::uint64_t>(starts_per_problem);
+  amp += static_cast<long long>(global / static_cast<std::uint64_t>(starts_per_problem)) * amp_stride;
   w += blockIdx.y * n;
   QPB_FOR(i, n) {
     const float phase = kTwoPi * uniform(seed, start, static_cast<std::uint64_t>(i));
@@ -136,9 +142,13 @@ dim3 grid(long long n, int batch) {
 
 }  // namespace
 
-void random_wave(float2* w, const float* amplitude, long long n, int batch, std::uint64_t seed,
-                 std::uint64_t first_start, cudaStream_t stream) {
-  random_wave_kernel<<<grid(n, batch), kThreads, 0, stream>>>(w, amplitude, n, seed, first_start);
+void random_wave(float2* w, const float* amplitude, long long amp_stride, int starts_per_problem,
+                 long long n, int batch, std::uint64_t seed, std::uint64_t first_start,
+                 cudaStream_t stream) {
+  if (starts_per_problem < 1) throw std::logic_error("random_wave: starts_per_problem < 1");
+  random_wave_kernel<<<grid(n, batch), kThreads, 0, stream>>>(w, amplitude, amp_stride,
+                                                              starts_per_problem, n, seed,
+                                                              first_start);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }

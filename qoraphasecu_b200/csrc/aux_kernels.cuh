@@ -15,9 +15,12 @@ struct Dims3 {
   QPB_HD long long n() const { return static_cast<long long>(d0) * d1 * d2; }
 };
 
-// w[b][i] = amp[i] / sqrt(n) * exp(i kTwoPi uniform(seed, first_start + b, i)).
-void random_wave(float2* w, const float* amplitude, long long n, int batch, std::uint64_t seed,
-                 std::uint64_t first_start, cudaStream_t stream);
+// w[b][i] = A[i] / sqrt(n) * exp(i kTwoPi uniform(seed, k, i)) for global start
+// s = first_start + b of problem q = s / starts_per_problem, k = s mod
+// starts_per_problem, A = amplitude + q * amp_stride (kernels.cpp:104-117).
+void random_wave(float2* w, const float* amplitude, long long amp_stride, int starts_per_problem,
+                 long long n, int batch, std::uint64_t seed, std::uint64_t first_start,
+                 cudaStream_t stream);
 
 // x[b][i] = 0 outside support[b][i].
 void support_project(float2* x, const std::uint8_t* support, long long n, int batch,

@@ -7,13 +7,15 @@
 #include <cstring>
 #include <exception>
 #include <string>
+#include <vector>
 
 #include "../../include/qpb.h"
+#include "batch.hpp"
 #include "solver.hpp"
 
 struct qpb_solver {
-  qpb::Solver impl;
-  qpb_solver(const qpb::ProblemView& p, const qpb::SolverOptions& o) : impl(p, o) {}
+  qpb::BatchSolver impl;
+  qpb_solver(const std::vector<qpb::ProblemView>& p, const qpb::SolverOptions& o) : impl(p, o) {}
 };
 
 namespace {
@@ -174,44 +176,72 @@ qpb_status qpb_half_support(const uint8_t* support, int ndim, const int64_t* sha
   });
 }
 
+namespace {
+
+// The reference's make_solver checks (solver.cpp:61-78), made before any device work.
+qpb::SolverOptions options_of(const qpb_options* options) {
+  require(options != nullptr, "options is NULL");
+  if (options->starts < 1) throw qpb::InvalidArgument("starts must be >= 1");
+  if (options->sync_every < 1) throw qpb::InvalidArgument("sync_every must be >= 1");
+  if (options->batch < 0 || (options->batch > 0 && options->starts % options->batch != 0)) {
+    throw qpb::InvalidArgument("batch must divide starts");
+  }
+  if (options->variant != QPB_VARIANT_BATCHED && options->variant != QPB_VARIANT_PLAIN) {
+    throw qpb::InvalidArgument("unknown variant");
+  }
+  if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_RESIDENT) {
+    throw qpb::InvalidArgument("unknown schedule");
+  }
+  qpb::SolverOptions o;
+  o.starts = options->starts;
+  o.batch = options->batch;
+  o.seed = options->seed;
+  o.start = reinterpret_cast<const float2*>(options->start);
+  o.sync_every = options->sync_every;
+  o.variant = static_cast<qpb::Variant>(options->variant);
+  o.amp_storage = storage_of(options->amp_storage);
+  o.device = options->device;
+  o.stream = static_cast<cudaStream_t>(options->stream);
+  o.schedule = static_cast<qpb::Schedule>(options->schedule);
+  return o;
+}
+
+qpb::ProblemView made_problem(const qpb_problem* problem) {
+  const qpb::ProblemView v = view(problem);
+  qpb::dims_of(v);
+  if (!v.amplitude || !v.support) {
+    throw qpb::InvalidArgument("problem arrays do not match its shape; build it with make_problem");
+  }
+  return v;
+}
+
+}  // namespace
+
 qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out) {
   return guarded([&] {
     require(out != nullptr, "out is NULL");
     *out = nullptr;
-    require(options != nullptr, "options is NULL");
-    // The reference's make_solver checks (solver.cpp:61-78) come before any device work.
-    if (options->starts < 1) throw qpb::InvalidArgument("starts must be >= 1");
-    if (options->sync_every < 1) throw qpb::InvalidArgument("sync_every must be >= 1");
-    if (options->batch < 0 || (options->batch > 0 && options->starts % options->batch != 0)) {
-      throw qpb::InvalidArgument("batch must divide starts");
-    }
-    if (options->variant != QPB_VARIANT_BATCHED && options->variant != QPB_VARIANT_PLAIN) {
-      throw qpb::InvalidArgument("unknown variant");
-    }
-    if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_RESIDENT) {
-      throw qpb::InvalidArgument("unknown schedule");
-    }
-    const qpb::ProblemView v = view(problem);
-    qpb::dims_of(v);
-    if (!v.amplitude || !v.support) {
-      throw qpb::InvalidArgument("problem arrays do not match its shape; build it with make_problem");
-    }
-    qpb::SolverOptions o;
-    o.starts = options->starts;
-    o.batch = options->batch;
-    o.seed = options->seed;
-    o.start = reinterpret_cast<const float2*>(options->start);
-    o.sync_every = options->sync_every;
-    o.variant = static_cast<qpb::Variant>(options->variant);
-    o.amp_storage = storage_of(options->amp_storage);
-    o.device = options->device;
-    o.stream = static_cast<cudaStream_t>(options->stream);
-    o.schedule = static_cast<qpb::Schedule>(options->schedule);
+    const qpb::SolverOptions o = options_of(options);
+    const qpb::ProblemView v = made_problem(problem);
     if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
     qpb::trace("qpb_create: starts=%d batch=%d variant=%d shape=%lld,%lld,%lld", o.starts, o.batch,
                options->variant, v.shape[0], v.shape[1], v.shape[2]);
-    *out = new qpb_solver(v, o);
+    *out = new qpb_solver({v}, o);
     qpb::trace("qpb_create: solver %p ready", static_cast<void*>(*out));
+  });
+}
+
+qpb_status qpb_create_batch(const qpb_problem* problems, size_t n_problems,
+                            const qpb_options* options, qpb_solver** out) {
+  return guarded([&] {
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    require(problems != nullptr && n_problems > 0, "no problems");
+    const qpb::SolverOptions o = options_of(options);
+    std::vector<qpb::ProblemView> views;
+    for (size_t q = 0; q < n_problems; ++q) views.push_back(made_problem(problems + q));
+    if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
+    *out = new qpb_solver(views, o);
   });
 }
 

@@ -86,6 +86,29 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
   float2* __restrict__ wl = p.w + base;
   float2* __restrict__ xl = p.x + base;
   const float2* __restrict__ tw = p.twiddle;
+  // A row's T threads share a warp, so its exchanges need warp barriers only.
+  constexpr bool kWarpLocal = ROWS && T <= 32;
+
+  // Control values are read before the transform so that their latency hides
+  // behind it: the error row (thread 0 of a modulus pass) and the update
+  // coefficients.
+  [[maybe_unused]] double* err_slot = nullptr;
+  if constexpr (M == Mode::kMod || M == Mode::kGrad) {
+    if (tid == 0) {
+      const Ctrl* c = p.ctrl;
+      const int r = c->counters[p.group];
+      if (r < c->capacity) {
+        err_slot = c->errs + static_cast<long long>(r) * p.starts_total + p.start0 + batch_start;
+      }
+    }
+  }
+  [[maybe_unused]] float ca = p.coef_a, cb = p.coef_b;
+  if constexpr (M == Mode::kUpd) {
+    if (p.coef_from_ctrl) {
+      ca = p.ctrl->a;
+      cb = p.ctrl->b;
+    }
+  }
 
   // Inputs that do not depend on the transform go to shared memory by bulk
   // asynchronous copies issued first: the whole input tile of a row pass, the
@@ -118,13 +141,14 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
         if (tid == 0) {
           const long long line_in_start =
               line0 - static_cast<long long>(batch_start) * p.lines_per_start;
-          const AmpT* src = static_cast<const AmpT*>(p.amp) + line_in_start * L;
+          const AmpT* src = static_cast<const AmpT*>(p.amp) +
+                            amp_offset(p, p.start0 + batch_start) + line_in_start * L;
           bulk_g2s(sbase + St::kExchange, src, St::kSideA, bar);
         }
       } else {
         // one copy per element index j of the lines: LINES adjacent amplitudes
         const long long outer = line0 / p.S;
-        const AmpT* src = static_cast<const AmpT*>(p.amp) +
+        const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
                           (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
         constexpr int kRowBytes = G::LINES * static_cast<int>(sizeof(AmpT));
         for (int j = tid; j < L; j += G::NT) {
@@ -166,7 +190,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
   }
 
   constexpr bool kStartsInverse = M == Mode::kInv || M == Mode::kUpd;
-  transform<L, kStartsInverse>(v, t, tw, row);
+  transform<L, kStartsInverse, kWarpLocal>(v, t, tw, row);
 
   if constexpr (St::kAmp) {
     if (!staged()) return;
@@ -183,21 +207,9 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
       v[m] = pointwise_projection<M>(v[m], a, s, acc);
     }
     const double total = block_sum_double(static_cast<double>(acc));
-    if (tid == 0) {
-      Ctrl* c = p.ctrl;
-      const int r = c->counters[p.group];
-      if (r < c->capacity) {
-        atomicAdd(&c->errs[static_cast<long long>(r) * p.starts_total + p.start0 + batch_start],
-                  total);
-      }
-    }
-    transform<L, true>(v, t, tw, row);
+    if (tid == 0 && err_slot) atomicAdd(err_slot, total);
+    transform<L, true, kWarpLocal>(v, t, tw, row);
   } else if constexpr (M == Mode::kUpd) {
-    float ca = p.coef_a, cb = p.coef_b;
-    if (p.coef_from_ctrl) {
-      ca = p.ctrl->a;
-      cb = p.ctrl->b;
-    }
     if constexpr (St::kUpd) {
       // x_new replaces the old iterate in its tile and leaves by one bulk store.
       float2* x_tile = reinterpret_cast<float2*>(sbase + St::kExchange);
@@ -234,7 +246,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
       __syncthreads();
     }
     if (p.bump_counter && blockIdx.x == 0 && tid == 0) ++p.ctrl->counters[p.group];
-    transform<L, false>(v, t, tw, row);
+    transform<L, false, kWarpLocal>(v, t, tw, row);
   } else if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
     const float inv_l = 1.0f / static_cast<float>(L);
 #pragma unroll
@@ -243,12 +255,13 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
       const float f = fftfreq(static_cast<std::uint32_t>(j), static_cast<std::uint32_t>(L));
       v[m] = cscale(v[m], expf(p.blur_k * f * f) * inv_l);
     }
-    transform<L, true>(v, t, tw, row);
+    transform<L, true, kWarpLocal>(v, t, tw, row);
   }
 
   if constexpr (St::kRowTma) {
-    // The transform's last stage ran in registers after a barrier, so region W
-    // is free: the output tile goes there and leaves by one bulk store.
+    // Region W is free once every warp is past its last exchange: the output
+    // tile goes there and leaves by one bulk store.
+    if constexpr (kWarpLocal) __syncthreads();
 #pragma unroll
     for (int m = 0; m < E; ++m) wtile[l * L + t + T * m] = v[m];
     fence_proxy_async();

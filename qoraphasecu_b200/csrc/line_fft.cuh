@@ -54,10 +54,21 @@ __device__ __forceinline__ void butterfly(float2* u) {
   }
 }
 
+// Orders a line's exchange: a block barrier, or a warp barrier when the
+// line's T threads share one warp (WARP_LOCAL) and no other warp uses its row.
+template <bool WARP_LOCAL>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (WARP_LOCAL) {
+    __syncwarp();
+  } else {
+    __syncthreads();
+  }
+}
+
 // One Stockham stage of radix R over the thread's E registers. NS is the
 // product of the radices before it; LAST stages leave values in place,
 // others exchange through the line's shared-memory row.
-template <int L, int R, int NS, bool LAST, bool INV>
+template <int L, int R, int NS, bool LAST, bool INV, bool WARP_LOCAL = false>
 __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
                                       const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
@@ -90,26 +101,31 @@ __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
     }
   }
   if constexpr (!LAST) {
-    __syncthreads();
+    line_sync<WARP_LOCAL>();
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = row[swz(t + T * m)];
-    __syncthreads();
+    line_sync<WARP_LOCAL>();
   }
 }
 
-template <int L, bool INV>
+// Forward (INV false) or inverse unnormalised transform of the line held in
+// v. With WARP_LOCAL the caller guarantees that the line's threads share a
+// warp (T <= 32, lines not straddling warps) and that no other warp touches
+// `row` during the call; then only warp barriers separate the stages.
+template <int L, bool INV, bool WARP_LOCAL = false>
 __device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
                                           const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
+  static_assert(!WARP_LOCAL || G::T <= 32, "a line spans several warps");
   if constexpr (G::STAGES == 1) {
-    stage<L, G::R0, 1, true, INV>(v, t, tw, row);
+    stage<L, G::R0, 1, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else if constexpr (G::STAGES == 2) {
-    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
-    stage<L, G::R1, G::R0, true, INV>(v, t, tw, row);
+    stage<L, G::R0, 1, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R1, G::R0, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else {
-    stage<L, G::R0, 1, false, INV>(v, t, tw, row);
-    stage<L, G::R1, G::R0, false, INV>(v, t, tw, row);
-    stage<L, G::R2, G::R0 * G::R1, true, INV>(v, t, tw, row);
+    stage<L, G::R0, 1, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R1, G::R0, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R2, G::R0 * G::R1, true, INV, WARP_LOCAL>(v, t, tw, row);
   }
 }
 

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(const PassParams p)
     for (int idx = threadIdx.x; idx < tile; idx += blockDim.x) {
       int l, j;
       tile_coords(p, idx, l, j);
-      const long long e = element(p, line0 + l, j) - start_off;
+      const long long e = element(p, line0 + l, j) - start_off + amp_offset(p, p.start0 + batch_start);
       const float a = load_amp<AmpT>(p.amp, e);
       res[l * ldl + j] = pointwise_projection<M>(res[l * ldl + j], a, s, acc);
     }

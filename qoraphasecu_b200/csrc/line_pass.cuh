@@ -55,6 +55,10 @@ struct PassParams {
   float2* w;
   float2* x;
   const void* amp;                // signed amplitude (-1 masked), FFT order, one per problem
+  // Several problems of one shape: the amplitude of global start s is at
+  // amp + (s / starts_per_problem) * amp_stride elements (amp_stride 0: one problem).
+  long long amp_stride;
+  int starts_per_problem;
   const std::uint8_t* support;    // [batch][n]
   Ctrl* ctrl;
   LevelAcc* level;                // [batch], kBlur with level != 0
@@ -82,6 +86,11 @@ struct PassParams {
   // pass (tile_amplitude) instead of FFT order: one contiguous tile per CTA.
   int amp_tiled;
 };
+
+// Element offset of the amplitude that global start `start` reads.
+QPB_HD long long amp_offset(const PassParams& p, int start) {
+  return p.amp_stride ? static_cast<long long>(start / p.starts_per_problem) * p.amp_stride : 0;
+}
 
 // Launches one generic line pass on `stream`.
 void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream);

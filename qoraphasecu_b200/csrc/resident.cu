@@ -16,7 +16,8 @@
 //     back and scatters the columns to where they came from;
 //   row phase: each CTA transforms its rows of ws back along x (= P_M x),
 //     applies the update x <- S ? P : a x + b P in xs and transforms the new
-//     iterate forward into ws.
+//     iterate forward into ws. A row's threads share one warp and its exchange
+//     reuses its own ws row, so the row transforms need warp barriers only.
 // Cluster barriers separate the phases. The chunk starts from x (the forward
 // row transforms are recomputed) and ends by writing x and w = FFT_x(x) to HBM,
 // which keeps the invariant of the streamed passes: shrinkwrap, detwin and
@@ -144,12 +145,15 @@ __global__ void __launch_bounds__(Resident<N>::NT, 1) resident_kernel(const Resi
     v[m] = p.x[rows_off + j];
     xs[j] = v[m];
   }
-  transform<N, false>(v, rt, tw, ws + rl * P);
+  transform<N, false, true>(v, rt, tw, ws + rl * P);
 #pragma unroll
   for (int m = 0; m < E; ++m) ws[rl * P + rt + T * m] = v[m];
 
   const unsigned ws_addr = smem_addr(ws);
-  const AmpT* __restrict__ amp = static_cast<const AmpT*>(p.amp);
+  const AmpT* __restrict__ amp =
+      static_cast<const AmpT*>(p.amp) +
+      (p.amp_stride ? static_cast<long long>((p.start0 + start) / p.starts_per_problem) * p.amp_stride
+                    : 0);
   const float scale = p.scale;
   for (int it = 0; it < p.iterations; ++it) {
     group_barrier<C>();  // every CTA's rows are transformed along x
@@ -195,7 +199,7 @@ __global__ void __launch_bounds__(Resident<N>::NT, 1) resident_kernel(const Resi
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = ws[rl * P + rt + T * m];
     __syncwarp();  // a row's threads share one warp; its exchange reuses the row
-    transform<N, true>(v, rt, tw, ws + rl * P);
+    transform<N, true, true>(v, rt, tw, ws + rl * P);
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const int j = rl * N + rt + T * m;
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(Resident<N>::NT, 1) resident_kernel(const Resi
       xs[j] = xn;
       v[m] = xn;
     }
-    transform<N, false>(v, rt, tw, ws + rl * P);
+    transform<N, false, true>(v, rt, tw, ws + rl * P);
 #pragma unroll
     for (int m = 0; m < E; ++m) ws[rl * P + rt + T * m] = v[m];
   }

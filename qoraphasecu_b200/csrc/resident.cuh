@@ -15,6 +15,8 @@ struct ResidentParams {
   float2* x;                     // [starts][n] iterate, FFT order (read at start, written at end)
   float2* w;                     // [starts][n] x-axis transform of x (written at end)
   const void* amp;               // signed amplitude (-1 masked), FFT order, [n], amp_storage type
+  long long amp_stride;          // elements between problems' amplitudes (0: one problem)
+  int starts_per_problem;
   const std::uint8_t* support;   // [starts][n]
   Ctrl* ctrl;                    // coefficients, error rows, counters[group] = first error row
   const float2* twiddle;         // W_N^k, k < N

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 
 #include "fast_pass.cuh"
@@ -230,6 +231,8 @@ PassParams PassRunner::params(Mode mode, int axis3, int batch) const {
   for (int s = 0; s < plan.stages; ++s) p.radix[s] = plan.radix[s];
   p.twiddle = plan.twiddle;
   p.scale = 1.0f / std::sqrt(static_cast<float>(p.n));
+  p.amp_stride = 0;
+  p.starts_per_problem = 1;
   return p;
 }
 
@@ -240,10 +243,15 @@ void PassRunner::launch(Mode mode, int axis3, PassParams p, cudaStream_t s) cons
 
 // ---------------------------------------------------------------------- Solver
 Solver::Solver(const ProblemView& problem, const SolverOptions& options)
-    : d_(dims_of(problem)),
-      ndim_(problem.ndim),
+    : Solver(std::vector<ProblemView>{problem}, options) {}
+
+Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& options)
+    : d_(dims_of(problems.at(0))),
+      ndim_(problems[0].ndim),
       n_(d_.n()),
-      starts_(options.starts),
+      problems_(static_cast<int>(problems.size())),
+      spp_(options.starts),
+      starts_(options.starts * static_cast<int>(problems.size())),
       batch_(1),
       groups_(1),
       options_(options),
@@ -252,12 +260,19 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
       runner_(d_, ndim_, plans_) {
   if (options.starts < 1) throw InvalidArgument("starts must be >= 1");
   if (options.sync_every < 1) throw InvalidArgument("sync_every must be >= 1");
-  if (options.batch < 0 || (options.batch > 0 && options.starts % options.batch != 0)) {
+  if (options.batch < 0 || (options.batch > 0 && starts_ % options.batch != 0)) {
     throw InvalidArgument("batch must divide starts");
   }
-  if (!problem.amplitude || !problem.support) {
-    throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
+  for (const ProblemView& q : problems) {
+    if (!q.amplitude || !q.support) {
+      throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
+    }
+    const Dims3 dq = dims_of(q);
+    if (q.ndim != ndim_ || dq.d0 != d_.d0 || dq.d1 != d_.d1 || dq.d2 != d_.d2) {
+      throw InvalidArgument("problems of one solver must share a shape");
+    }
   }
+  const ProblemView& problem = problems[0];
   const bool resident_ok = resident_supports(problem.ndim, d_.d1, d_.d2);
   if (options.schedule == Schedule::kResident) {
     if (options.variant == Variant::kPlain) {
@@ -274,7 +289,9 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   } else if (options.batch) {
     batch_ = options.batch;
   } else if (options.tune) {
+    // Tuned on the first problem with every start: the work is the same.
     SolverOptions o = options;
+    o.starts = starts_;
     if (!resident_ok) o.schedule = Schedule::kStreamed;
     const TunedSchedule t = tuned_schedule(problem, o);
     batch_ = t.batch;
@@ -286,30 +303,38 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   groups_ = starts_ / batch_;
   if (resident_) configure_resident();
   options_.start = nullptr;
+  amp_stride_ = problems_ > 1 ? n_ : 0;
 
-  const auto amp = host_roll(problem.amplitude, d_, true);
-  std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
-  if (problem.mask) {
-    mask = host_roll(problem.mask, d_, true);
-    for (auto& m : mask) m = m != 0;
-  }
-  auto sup = host_roll(problem.support, d_, true);
-  for (auto& s : sup) s = s != 0;
-  energy_ = usable_energy(amp, mask);
-  {
-    // The amplitude is read by the modulus pass only; when that pass runs the
-    // register-resident kernel, store it in the kernel's CTA order so each CTA
-    // stages its tile with one bulk copy.
+  // Per problem: FFT-order amplitude, mask, support; signed amplitude in the
+  // storage type (in the modulus pass's CTA order when that pass runs the
+  // register-resident kernel, so each CTA stages its tile with one bulk copy).
+  const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
+  const int lines = fast_pass_lines(mod);
+  const bool tile = lines > 0 && mod.S > 1 && !resident_;
+  std::vector<float> amp_all;
+  std::vector<unsigned char> signed_all;
+  std::vector<std::vector<std::uint8_t>> supports;
+  for (const ProblemView& q : problems) {
+    const auto amp = host_roll(q.amplitude, d_, true);
+    std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
+    if (q.mask) {
+      mask = host_roll(q.mask, d_, true);
+      for (auto& m : mask) m = m != 0;
+    }
+    auto sup = host_roll(q.support, d_, true);
+    for (auto& v : sup) v = v != 0;
+    energies_.push_back(usable_energy(amp, mask));
     auto bytes = signed_amplitude(amp, mask, options.amp_storage);
-    const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
-    const int lines = fast_pass_lines(mod);
-    if (lines > 0 && mod.S > 1 && !resident_) {
+    if (tile) {
       const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
       bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
-      amp_tiled_ = true;
     }
-    amp_ = upload(bytes, stream_);
+    amp_all.insert(amp_all.end(), amp.begin(), amp.end());
+    signed_all.insert(signed_all.end(), bytes.begin(), bytes.end());
+    supports.push_back(std::move(sup));
   }
+  amp_tiled_ = tile;
+  amp_ = upload(signed_all, stream_);
 
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
   x_ = DeviceBuffer<float2>(total);
@@ -324,11 +349,16 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
   const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
   set_ctrl(ctrl_.get(), ctrl, stream_);
-  QPB_CHECK(cudaMemcpyAsync(support_.get(), sup.data(), sup.size(), cudaMemcpyHostToDevice, stream_));
-  for (int s = 1; s < starts_; ++s) {
-    QPB_CHECK(cudaMemcpyAsync(support_.get() + static_cast<std::size_t>(s) * n_, support_.get(),
-                              static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
+  for (int q = 0; q < problems_; ++q) {
+    std::uint8_t* first = support_.get() + static_cast<std::size_t>(q) * spp_ * n_;
+    QPB_CHECK(cudaMemcpyAsync(first, supports[q].data(), supports[q].size(),
+                              cudaMemcpyHostToDevice, stream_));
+    for (int s = 1; s < spp_; ++s) {
+      QPB_CHECK(cudaMemcpyAsync(first + static_cast<std::size_t>(s) * n_, first,
+                                static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
+    }
   }
+  stream_.sync();  // the host vectors above are released at the end of this scope
   errors_.assign(static_cast<std::size_t>(starts_), {});
 
   if (options.start) {
@@ -342,9 +372,9 @@ Solver::Solver(const ProblemView& problem, const SolverOptions& options)
   } else {
     // Random phases on the measured amplitude, inverse transform, cut to the
     // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
-    auto amp_f = upload(amp, stream_);
+    auto amp_f = upload(amp_all, stream_);
     for (int g = 0; g < groups_; ++g) {
-      random_wave(w(g), amp_f.get(), n_, batch_, options.seed,
+      random_wave(w(g), amp_f.get(), amp_stride_, spp_, n_, batch_, options.seed,
                   static_cast<std::uint64_t>(g) * batch_, stream_);
       const int outer = runner_.outer();
       runner_.launch(Mode::kInv, outer, base(Mode::kInv, outer, g), stream_);
@@ -384,6 +414,8 @@ PassParams Solver::base(Mode mode, int axis3, int g) const {
   p.bump_counter = 1;
   p.amp_storage = options_.amp_storage;
   p.amp_tiled = amp_tiled_ && mode == Mode::kMod ? 1 : 0;
+  p.amp_stride = amp_stride_;
+  p.starts_per_problem = spp_;
   return p;
 }
 
@@ -413,6 +445,8 @@ void Solver::enqueue_chunk(int len, cudaStream_t s) {
   p.x = x_.get();
   p.w = w_.get();
   p.amp = amp_.get();
+  p.amp_stride = amp_stride_;
+  p.starts_per_problem = spp_;
   p.support = support_.get();
   p.ctrl = ctrl_.get();
   p.twiddle = runner_.params(Mode::kFwd, 2, starts_).twiddle;
@@ -425,7 +459,7 @@ void Solver::enqueue_chunk(int len, cudaStream_t s) {
   launch_resident(p, d_.d2, starts_, s);
 }
 
-void Solver::run(const OpDesc* ops, std::size_t count) {
+void Solver::begin_run(const OpDesc* ops, std::size_t count) {
   validate_recipe(ops, count);
   for (std::size_t i = 0; i < count; ++i) {
     if (ops[i].kind == kOpDetwinBegin && (ops[i].axis < 0 || ops[i].axis >= ndim_)) {
@@ -441,10 +475,33 @@ void Solver::run(const OpDesc* ops, std::size_t count) {
   set_ctrl(ctrl_.get(), ctrl, stream_);
   QPB_CHECK(cudaMemsetAsync(errs_.get(), 0, needed * sizeof(double), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
-  trace("run: control block written");
   stream_.sync();
-  trace("run: synchronized");
   run_iterations_ = 0;
+}
+
+void Solver::apply(const OpDesc& o) {
+  switch (o.kind) {
+    case kOpShrinkwrap:
+      shrinkwrap(o);
+      break;
+    case kOpDetwinBegin:
+      detwin_begin(o.axis);
+      break;
+    case kOpDetwinEnd:
+      detwin_end();
+      break;
+    default:
+      throw std::logic_error("Solver::apply: not a support operation");
+  }
+}
+
+void Solver::end_run() {
+  collect_errors(run_iterations_);
+  check_waits();
+}
+
+void Solver::run(const OpDesc* ops, std::size_t count) {
+  begin_run(ops, count);
   for (std::size_t i = 0; i < count; ++i) {
     const OpDesc& o = ops[i];
     trace("run op %zu/%zu kind=%d n=%d (iteration %d)", i, count, o.kind, o.n, iteration_);
@@ -458,58 +515,76 @@ void Solver::run(const OpDesc* ops, std::size_t count) {
       case kOpRAAR:
         iterate(o.n, raar_coefficients(o.beta));
         break;
-      case kOpShrinkwrap:
-        shrinkwrap(o);
-        break;
-      case kOpDetwinBegin:
-        detwin_begin(o.axis);
-        break;
-      case kOpDetwinEnd:
-        detwin_end();
+      default:
+        apply(o);
         break;
     }
   }
-  collect_errors(run_iterations_);
-  check_waits();
+  end_run();
+}
+
+void Solver::begin_iterate(Coefficients c) {
+  if (!wave_valid_) establish_wave();
+  set_coefficients(ctrl_.get(), c.a, c.b, stream_);
+}
+
+int Solver::chunk_length(int remaining) const {
+  const int every = options_.sync_every;
+  return std::min(remaining, every - iteration_ % every);
+}
+
+void Solver::prepare_branches() {
+  if (groups_ > 1 && branches_.empty() && options_.variant == Variant::kBatched && !resident_) {
+    // one branch stream per group plus a fork event and a join event per group
+    for (int g = 0; g < groups_; ++g) branches_.push_back(std::make_unique<Stream>());
+    branch_events_.resize(static_cast<std::size_t>(groups_) + 1);
+    for (auto& e : branch_events_) QPB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+}
+
+// `len` iterations of every start, enqueued on `s` (captured into a graph by
+// the batched variant): the resident kernel, or the groups' passes, each group
+// a parallel branch so that one group's modulus pass can overlap another
+// group's update pass; the plain variant runs groups one after another.
+void Solver::enqueue_chunk_body(int len, cudaStream_t s) {
+  if (resident_) {
+    enqueue_chunk(len, s);
+  } else if (groups_ > 1 && options_.variant == Variant::kBatched) {
+    if (branches_.empty()) throw std::logic_error("prepare_branches() was not called");
+    QPB_CHECK(cudaEventRecord(branch_events_[0], s));
+    for (int g = 0; g < groups_; ++g) {
+      cudaStream_t b = *branches_[g];
+      QPB_CHECK(cudaStreamWaitEvent(b, branch_events_[0], 0));
+      for (int i = 0; i < len; ++i) enqueue_iteration(g, b);
+      QPB_CHECK(cudaEventRecord(branch_events_[g + 1], b));
+      QPB_CHECK(cudaStreamWaitEvent(s, branch_events_[g + 1], 0));
+    }
+  } else {
+    for (int g = 0; g < groups_; ++g) {
+      for (int i = 0; i < len; ++i) enqueue_iteration(g, s);
+    }
+  }
+}
+
+void Solver::end_chunk(int len) {
+  iteration_ += len;
+  run_iterations_ += len;
+  if (progress_ && iteration_ % options_.sync_every == 0) report();
 }
 
 void Solver::iterate(int count, Coefficients c) {
-  if (!wave_valid_) establish_wave();
-  set_coefficients(ctrl_.get(), c.a, c.b, stream_);
-  const int every = options_.sync_every;
+  begin_iterate(c);
   for (int done = 0; done < count;) {
-    const int len = std::min(count - done, every - iteration_ % every);
+    const int len = chunk_length(count - done);
     if (options_.variant == Variant::kBatched) {
       auto it = graphs_.find(len);
       trace("iterate chunk len=%d graph=%s", len, it == graphs_.end() ? "capture" : "cached");
       if (it == graphs_.end()) {
+        prepare_branches();
         const unsigned long long before = launches();
-        if (groups_ > 1 && branches_.empty()) {
-          // one branch stream per group plus a fork event and a join event per group
-          for (int g = 0; g < groups_; ++g) branches_.push_back(std::make_unique<Stream>());
-          branch_events_.resize(static_cast<std::size_t>(groups_) + 1);
-          for (auto& e : branch_events_) {
-            QPB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-          }
-        }
         QPB_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
-          if (groups_ > 1) {
-            // Independent start groups become parallel branches of the graph, so
-            // one group's modulus pass can overlap another group's update pass.
-            QPB_CHECK(cudaEventRecord(branch_events_[0], stream_));
-            for (int g = 0; g < groups_; ++g) {
-              cudaStream_t s = *branches_[g];
-              QPB_CHECK(cudaStreamWaitEvent(s, branch_events_[0], 0));
-              for (int i = 0; i < len; ++i) enqueue_iteration(g, s);
-              QPB_CHECK(cudaEventRecord(branch_events_[g + 1], s));
-              QPB_CHECK(cudaStreamWaitEvent(stream_, branch_events_[g + 1], 0));
-            }
-          } else if (resident_) {
-            enqueue_chunk(len, stream_);
-          } else {
-            for (int i = 0; i < len; ++i) enqueue_iteration(0, stream_);
-          }
+          enqueue_chunk_body(len, stream_);
         } catch (...) {
           cudaGraph_t broken{};
           cudaStreamEndCapture(stream_, &broken);
@@ -524,14 +599,10 @@ void Solver::iterate(int count, Coefficients c) {
       }
       it->second->launch(stream_);
     } else {
-      for (int g = 0; g < groups_; ++g) {
-        for (int i = 0; i < len; ++i) enqueue_iteration(g, stream_);
-      }
+      enqueue_chunk_body(len, stream_);
     }
+    end_chunk(len);
     done += len;
-    iteration_ += len;
-    run_iterations_ += len;
-    if (progress_ && iteration_ % every == 0) report();
   }
 }
 
@@ -627,8 +698,8 @@ void Solver::detwin_end() {
   QPB_CHECK(cudaMemcpyAsync(support_.get(), saved_.get(), total, cudaMemcpyDeviceToDevice, stream_));
 }
 
-float Solver::to_error(double num) const {
-  return static_cast<float>(std::sqrt(num / (energy_ + kEps)));
+float Solver::to_error(double num, int start) const {
+  return static_cast<float>(std::sqrt(num / (energies_[start / spp_] + kEps)));
 }
 
 void Solver::collect_errors(int iterations) {
@@ -642,19 +713,25 @@ void Solver::collect_errors(int iterations) {
   stream_.sync();
   for (int t = 0; t < iterations; ++t) {
     for (int s = 0; s < starts_; ++s) {
-      errors_[s].push_back(to_error(host_errs_[static_cast<std::size_t>(t) * starts_ + s]));
+      errors_[s].push_back(to_error(host_errs_[static_cast<std::size_t>(t) * starts_ + s], s));
     }
   }
 }
 
-void Solver::report() {
+std::vector<float> Solver::latest_errors() {
+  if (run_iterations_ < 1) throw std::logic_error("latest_errors before any iteration");
   std::vector<double> row(static_cast<std::size_t>(starts_));
   QPB_CHECK(cudaMemcpyAsync(row.data(),
                             errs_.get() + static_cast<std::size_t>(run_iterations_ - 1) * starts_,
                             row.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   stream_.sync();
   std::vector<float> latest(row.size());
-  for (std::size_t s = 0; s < row.size(); ++s) latest[s] = to_error(row[s]);
+  for (std::size_t s = 0; s < row.size(); ++s) latest[s] = to_error(row[s], static_cast<int>(s));
+  return latest;
+}
+
+void Solver::report() {
+  const std::vector<float> latest = latest_errors();
   progress_(progress_user_, iteration_, latest.data(), starts_);
 }
 

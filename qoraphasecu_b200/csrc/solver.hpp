@@ -181,9 +181,24 @@ class PassRunner {
   const LinePlan* plans_[3];
 };
 
+// DeviceSelect makes `requested` (>= 0) the calling thread's device before any
+// allocation and remembers the device in use.
+struct DeviceSelect {
+  int device = 0;
+  explicit DeviceSelect(int requested) {
+    if (requested >= 0) QPB_CHECK(cudaSetDevice(requested));
+    QPB_CHECK(cudaGetDevice(&device));
+  }
+};
+
+// Several problems of one shape may share a solver: options.starts starts per
+// problem, problem q's starts at q * starts, each with its own amplitude,
+// mask, support and error normalisation, random starts keyed as if the
+// problem ran alone.
 class Solver {
  public:
   Solver(const ProblemView& problem, const SolverOptions& options);
+  Solver(const std::vector<ProblemView>& problems, const SolverOptions& options);
   ~Solver();
   Solver(const Solver&) = delete;
   Solver& operator=(const Solver&) = delete;
@@ -191,10 +206,13 @@ class Solver {
   void run(const OpDesc* ops, std::size_t count);
   std::size_t error_count() const { return errors_.empty() ? 0 : errors_[0].size(); }
   int starts() const { return starts_; }
+  int problems() const { return problems_; }
   bool resident() const { return resident_; }
   int batch() const { return batch_; }
   long long numel() const { return n_; }
+  int ndim() const { return ndim_; }
   int device() const { return select_.device; }
+  cudaStream_t stream() const { return stream_; }
   // objects: starts * numel complex64; supports: starts * numel; errors: starts * error_count().
   void results(float2* objects, std::uint8_t* supports, float* errors);
   void set_progress(ProgressFn fn, void* user) {
@@ -205,6 +223,22 @@ class Solver {
   // CUDA events; ms[p] receives the mean duration of pass p of an iteration.
   // Returns the number of passes per iteration (at most 8). Advances the state.
   int profile_passes(int iterations, double* ms);
+
+  // The steps of run(), for a driver that captures the chunks of several
+  // solvers on one stream into one graph (BatchSolver):
+  //   begin_run; per op: iterations -> begin_iterate, then per chunk
+  //   chunk_length / prepare_branches / enqueue_chunk_body (captured) / end_chunk;
+  //   other ops -> apply; finally end_run.
+  void begin_run(const OpDesc* ops, std::size_t count);
+  void begin_iterate(Coefficients c);
+  int chunk_length(int remaining) const;
+  void prepare_branches();
+  void enqueue_chunk_body(int len, cudaStream_t s);
+  void end_chunk(int len);
+  void apply(const OpDesc& o);
+  void end_run();
+  // The latest error of every start (after at least one iteration of this run).
+  std::vector<float> latest_errors();
 
  private:
   float2* x(int g) const { return x_.get() + static_cast<std::size_t>(g) * batch_ * n_; }
@@ -224,27 +258,23 @@ class Solver {
   void detwin_end();
   void collect_errors(int iterations);
   void report();
-  float to_error(double num) const;
+  float to_error(double num, int start) const;
 
   Dims3 d_;
   int ndim_;
   long long n_;
+  int problems_;
+  int spp_;  // starts per problem
   int starts_;
   int batch_;
   int groups_;
   SolverOptions options_;
-  // Selects the device before any allocation; every later call re-selects it.
-  struct DeviceSelect {
-    int device = 0;
-    explicit DeviceSelect(int requested) {
-      if (requested >= 0) QPB_CHECK(cudaSetDevice(requested));
-      QPB_CHECK(cudaGetDevice(&device));
-    }
-  } select_;
+  DeviceSelect select_;  // before any allocation; every later call re-selects it
   PlanCache plans_;
   Stream stream_;
   PassRunner runner_;
-  double energy_ = 0.0;
+  std::vector<double> energies_;     // usable energy per problem
+  long long amp_stride_ = 0;         // elements between problems' amplitudes in amp_
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
   bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
   bool resident_ = false;            // iterations run by the resident kernel

@@ -74,6 +74,29 @@ def test_create_validates_before_touching_a_device():
             _lib.check(status)
 
 
+def test_create_batch_validates_before_touching_a_device():
+    lib = _lib.load()
+    amp = np.ones((8, 8), np.float32)
+    sup = np.ones((8, 8), np.uint8)
+    p = qpc.api.Problem(amp, np.zeros((8, 8), np.uint8), sup)
+    views = (_lib.Problem * 2)(p._c(), p._c())
+    handle = ctypes.c_void_p()
+    o = _lib.Options(starts=2, batch=0, seed=0, start=None, sync_every=10, variant=0,
+                     amp_storage=0, device=-1, stream=None, schedule=0)
+    assert lib.qpb_create_batch(views, 0, ctypes.byref(o), ctypes.byref(handle)) == \
+        _lib.INVALID_ARGUMENT
+    assert "no problems" in lib.qpb_last_error().decode()
+    o.schedule = 7
+    assert lib.qpb_create_batch(views, 2, ctypes.byref(o), ctypes.byref(handle)) == \
+        _lib.INVALID_ARGUMENT
+    assert "unknown schedule" in lib.qpb_last_error().decode()
+    o.schedule = 0
+    views[1].ndim = 4
+    assert lib.qpb_create_batch(views, 2, ctypes.byref(o), ctypes.byref(handle)) == \
+        _lib.INVALID_ARGUMENT
+    assert handle.value is None
+
+
 def test_run_rejects_null_solver_and_bad_recipes():
     lib = _lib.load()
     ops = (_lib.Op * 1)(_lib.Op(0, 0, 0, 0, 0, 0, 0))

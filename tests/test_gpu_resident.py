@@ -112,4 +112,4 @@ def test_tuning_report_lists_the_resident_candidate(gpu):
         s.run(Recipe(ER(2)))
     report = qpc.api.tuning_report()
     lines = [l for l in report.splitlines() if "1x128x128 starts 4 " in l]
-    assert any("resident:" in l for l in lines)
+    assert any("resident (" in l and "clusters of 2 CTAs" in l for l in lines)
