@@ -35,11 +35,15 @@ SHAPE = (256, 256)
 STARTS = 32
 SEED = 1000
 WORKLOAD = "gaussians 256x256 complex64, 32 starts, repeat(10, RAAR(50,0.9), Shrinkwrap(0.3,1.0)), ER(200)"
-# Algorithmic bytes per element of each line pass (SURVEY 8d figures applied to
-# what each fused pass must move): modulus pass reads the wave and the FP32
-# amplitude and writes the wave; update pass reads the wave, support and old
-# iterate and writes the iterate and the next wave.
+# Algorithmic bytes per element of each fused line pass (what the pass must
+# move at least): the modulus pass reads the wave and the FP32 amplitude and
+# writes the wave; the update pass reads the wave, support and old iterate and
+# writes the iterate and the next wave.
 PASS_BYTES = {"modulus (y-axis fwd+P_M+inv)": 8 + 4 + 8, "update (x-axis inv+update+fwd)": 8 + 1 + 8 + 8 + 8}
+# What the same work moves as separate kernels (one FFT pass = 16 B per
+# element; modulus 20 B, update 25 B): the rate an unfused chain would need.
+UNFUSED_BYTES = {"modulus (y-axis fwd+P_M+inv)": 16 + 20 + 16,
+                 "update (x-axis inv+update+fwd)": 16 + 25 + 16}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -238,6 +242,160 @@ def run_profile_step(sync_every):
     return 0
 
 
+# ----------------------------------------------------- the other synthetic workloads
+def _timed(fn, warmup=1, reps=3):
+    """Median wall time of fn() after `warmup` calls (each call synchronises)."""
+    for _ in range(warmup):
+        fn()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times)
+
+
+def workload_square(args):
+    """64x64 square object (uniform amplitude and phase in a 24x24 box),
+    noiseless, no mask, autocorrelation support, default recipe (720
+    iterations), 8 starts, through the public reconstruct()."""
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+
+    obj = workloads.square(64, seed=0)
+    intensity = workloads.simulate_intensity(obj)
+    out = {}
+    for storage in ("f32", "f16", "bf16"):
+        ens = None
+
+        def run():
+            nonlocal ens
+            ens = qpc.reconstruct(intensity, starts=8, seed=0, amp_storage=storage)
+
+        s = _timed(run, warmup=args.warmup, reps=args.steps)
+        out[storage] = {"start_iterations_per_s": 8 * 720 / s, "seconds": s,
+                        "best_error": ens.best.error, "errors": [r.error for r in ens]}
+    return {"workload": "square 64x64, 8 starts, default_recipe (720 iterations), e2e reconstruct()",
+            "storage": out, "tuning": qpc.api.tuning_report().strip().splitlines()}
+
+
+def workload_uneven(args):
+    """64 problems with sides drawn from {64, 128, 256, 512}, square objects
+    scaled to the side, Poisson 1e6, beamstop n/32, 4 starts each, recipe
+    repeat(4, HIO(50), Shrinkwrap(rms 0.3)), ER(100), in one BatchSolver."""
+    import numpy as np
+
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+
+    batch = workloads.uneven_batch(count=64, seed=2000)
+    recipe = workloads.uneven_recipe()
+    problems = [qpc.make_problem(b[1], mask=b[2]) for b in batch]
+    sides = [int(b[1].shape[0]) for b in batch]
+    elements = sum(s * s for s in sides)
+    result = {}
+
+    def run():
+        with qpc.BatchSolver(problems, starts=4, seed=0, sync_every=50) as solver:
+            solver.run(recipe)
+            result["runs"] = solver.results()
+
+    s = _timed(run, warmup=args.warmup, reps=args.steps)
+    iters = recipe.iterations()
+    best = [min(r.error for r in runs) for runs in result["runs"]]
+    per_side = {}
+    for side, b in zip(sides, best):
+        per_side.setdefault(side, []).append(b)
+    return {
+        "workload": "uneven batch: 64 problems, sides {64,128,256,512}, 4 starts, "
+                    "repeat(4, HIO(50), Shrinkwrap(rms 0.3)), ER(100); each timed call builds "
+                    "one BatchSolver (uploads, random starts) and runs the recipe; the "
+                    "warm-up calls leave the autotuner's choices cached",
+        "problems_per_side": {str(k): len(v) for k, v in sorted(per_side.items())},
+        "seconds": s,
+        "start_iterations_per_s": 64 * 4 * iters / s,
+        "element_iterations_per_s": 4 * elements * iters / s,
+        "best_error_median_per_side": {str(k): float(np.median(v))
+                                       for k, v in sorted(per_side.items())},
+        "tuning": qpc.api.tuning_report().strip().splitlines(),
+    }
+
+
+def workload_adam(args):
+    """Differentiable reconstruction: one 512x512 square-object problem (box
+    192, Poisson 1e7, beamstop r 12), a batch of 16 objects (random starts),
+    500 Adam steps (lr 1e-2) on the amplitude loss with the support projection,
+    against RAAR(0.9) from the same starts for the same wall time."""
+    import numpy as np
+
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import autograd as qad
+    from qoraphasecu_b200 import workloads
+    from qoraphasecu_b200.recipe import RAAR, Recipe
+
+    rng = np.random.default_rng(4000)
+    obj = workloads.square(512, seed=4000)
+    intensity = workloads.poisson(workloads.simulate_intensity(obj), 1e7, rng)
+    problem = qpc.make_problem(intensity, mask=workloads.beamstop((512, 512), 12))
+    qad.adam_reconstruct(problem, starts=16, steps=5, seed=0)  # warm-up
+    t0 = time.perf_counter()
+    adam = qad.adam_reconstruct(problem, starts=16, steps=500, lr=1e-2, seed=0)
+    t_adam = time.perf_counter() - t0
+    with qpc.Solver(problem, starts=16, seed=0, sync_every=50) as s:
+        s.run(Recipe(RAAR(50, 0.9)))  # warm-up: tuning, graphs
+    with qpc.Solver(problem, starts=16, seed=0, sync_every=50) as s:
+        t0 = time.perf_counter()
+        s.run(Recipe(RAAR(100, 0.9)))
+        per_iter = (time.perf_counter() - t0) / 100
+    n_raar = max(1, int(t_adam / per_iter))
+    with qpc.Solver(problem, starts=16, seed=0, sync_every=50) as s:
+        t0 = time.perf_counter()
+        s.run(Recipe(RAAR(n_raar, 0.9)))
+        t_raar = time.perf_counter() - t0
+        raar = s.results()
+    return {
+        "workload": "square 512x512 (box 192), Poisson 1e7, beamstop r 12, 16 starts: "
+                    "Adam(lr 1e-2) x 500 on sum_unmasked (|Fx| - sqrt(I))^2 with support "
+                    "projection vs RAAR(0.9) for the same wall time",
+        "adam": {"steps": 500, "seconds": t_adam, "steps_per_s": 500 / t_adam,
+                 "final_error_median": float(np.median([r.error for r in adam])),
+                 "final_error_best": float(min(r.error for r in adam))},
+        "raar": {"iterations": n_raar, "seconds": t_raar,
+                 "final_error_median": float(np.median([r.error for r in raar])),
+                 "final_error_best": float(min(r.error for r in raar))},
+    }
+
+
+def workload_crystal(args):
+    """128^3 faceted crystal (12 half-spaces in a sphere of radius 40,
+    displacement-field phase), Poisson 1e7, no mask, autocorrelation support,
+    default recipe (720 iterations), 4 starts batched, FP32 and FP16 storage."""
+    import qoraphasecu_b200 as qpc
+    from qoraphasecu_b200 import workloads
+    from qoraphasecu_b200.recipe import default_recipe
+
+    _, intensity = workloads.crystal(128, seed=3000)
+    problem = qpc.make_problem(intensity)
+    out = {}
+    for storage in ("f32", "f16"):
+        with qpc.Solver(problem, starts=4, seed=0, sync_every=50, amp_storage=storage) as s:
+            s.run(default_recipe())  # warm-up: tuning, graphs
+            t0 = time.perf_counter()
+            s.run(default_recipe())
+            sec = time.perf_counter() - t0
+            runs = s.results()
+            pass_ms = s.profile_passes(5)
+        out[storage] = {"seconds": sec, "start_iterations_per_s": 4 * 720 / sec,
+                        "errors": [r.error for r in runs], "pass_ms": pass_ms}
+    return {"workload": "crystal 128^3, Poisson 1e7, 4 starts, default_recipe (720 iterations, "
+                        "continued from a first run)", "storage": out,
+            "tuning": qpc.api.tuning_report().strip().splitlines()}
+
+
+WORKLOADS = {"square": workload_square, "uneven": workload_uneven, "adam": workload_adam,
+             "crystal": workload_crystal}
+
+
 # ---------------------------------------------------------------------- our arm
 def main(argv=None):
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
@@ -255,6 +413,9 @@ def main(argv=None):
                         help="only build the workload and run ITERS RAAR iterations (for ncu)")
     parser.add_argument("--schedule", choices=("auto", "streamed", "resident"), default="auto",
                         help="batched schedule of the timed solver (auto = autotuned)")
+    parser.add_argument("--workload", choices=sorted(WORKLOADS), default=None,
+                        help="report one of the other synthetic workloads instead of the "
+                             "benchmark line (--steps timed runs after --warmup)")
     parser.add_argument("--profile-step", action="store_true",
                         help="only build the workload and run one benchmark step (for ncu)")
     args = parser.parse_args(argv)
@@ -262,6 +423,9 @@ def main(argv=None):
         return run_profile(args.profile, "resident" if args.schedule == "resident" else "streamed")
     if args.profile_step:
         return run_profile_step(args.sync_every)
+    if args.workload:
+        print(json.dumps({"workload_report": args.workload, **WORKLOADS[args.workload](args)}))
+        return 0
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
@@ -340,13 +504,15 @@ def main(argv=None):
     elems = STARTS * SHAPE[0] * SHAPE[1]
     passes = []
     for (name, bpe), ms in zip(PASS_BYTES.items(), pass_ms):
-        passes.append({"pass": name, "ms": ms, "bytes": bpe * elems, "gbs": bpe * elems / (ms * 1e6)})
+        unfused = UNFUSED_BYTES[name] * elems
+        passes.append({"pass": name, "ms": ms, "bytes": bpe * elems, "gbs": bpe * elems / (ms * 1e6),
+                       "unfused_equivalent_gbs": unfused / (ms * 1e6)})
     dominant = max(passes, key=lambda p: p["ms"])
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
     # The whole iteration in the timed graph (parallel start groups, shrinkwrap
-    # amortised): minimum 21 B per element per iteration and the
-    # bytes the two fused passes move.
+    # amortised): the minimum 21 B per element per iteration (iterate in and
+    # out, amplitude, support) and the bytes the two fused passes move.
     iter_ms = total_ms / args.steps / iters
     fused_bytes = sum(PASS_BYTES.values()) * elems
     roofline = {

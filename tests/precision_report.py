@@ -1,0 +1,184 @@
+#!/usr/bin/env python3
+"""Error of the B200 backend against the FP64 oracle on every synthetic
+workload, for FP32, FP16 and BF16 amplitude storage. Needs a GPU; prints one
+JSON line per workload.
+
+    python tests/precision_report.py [--full] [--only NAME ...]
+
+For each workload and storage: a prefix of iterations from the same seeds
+(the random starts are bit-identical by construction) compared start by start
+with the oracle -- the largest relative difference of the per-iteration
+Fourier errors and the relative L2 difference of the objects -- and, where
+the oracle finishes in about a minute (or everywhere with --full), the whole
+recipe: the best start's final Fourier error and its object error against the
+ground truth after phase-ramp and twin alignment, each beside the oracle's.
+Iterative recipes are chaotic (long runs from one start diverge at rounding
+level), so whole recipes are compared through those two numbers.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parent))
+
+from oracle import fp64  # noqa: E402
+
+import qoraphasecu_b200 as qpc  # noqa: E402
+from qoraphasecu_b200 import autograd as qad  # noqa: E402
+from qoraphasecu_b200 import workloads  # noqa: E402
+from qoraphasecu_b200.recipe import HIO, RAAR, Recipe, default_recipe  # noqa: E402
+
+STORAGES = ("f32", "f16", "bf16")
+WORKERS = len(os.sched_getaffinity(0))
+
+
+def oracle_runs(intensity, support, mask, ops, starts, seed=0):
+    problem = fp64.make_problem(intensity, support, mask)
+    solver = fp64.Solver(problem, starts=starts, seed=seed, fft="scipy", workers=WORKERS)
+    solver.run(ops)
+    return solver.results()
+
+
+def gpu_runs(problem, recipe, starts, storage, seed=0):
+    with qpc.Solver(problem, starts=starts, seed=seed, amp_storage=storage, sync_every=50) as s:
+        s.run(recipe)
+        return s.results()
+
+
+def prefix(intensity, support, mask, recipe, starts):
+    """Start-by-start comparison over a short recipe, per storage."""
+    ref = oracle_runs(intensity, support, mask, recipe.ops(), starts)
+    problem = qpc.make_problem(intensity, support=support, mask=mask)
+    out = {}
+    for storage in STORAGES:
+        ours = gpu_runs(problem, recipe, starts, storage)
+        err = max(float(np.max(np.abs(r.errors - e) / np.maximum(e, 1e-12)))
+                  for (_, _, e), r in zip(ref, ours))
+        obj = max(fp64.relative_diff(r.object, o) for (o, _, _), r in zip(ref, ours))
+        out[storage] = {"max_rel_error_diff": err, "max_object_rel_l2": obj}
+    return {"recipe": repr(recipe.ops()), "starts": starts, "storage": out}
+
+
+def whole(intensity, support, mask, recipe, starts, truth):
+    """Best start's final error and aligned object error, ours beside the oracle's."""
+    t0 = time.perf_counter()
+    ref = oracle_runs(intensity, support, mask, recipe.ops(), starts)
+    ref_seconds = time.perf_counter() - t0
+    best = min(ref, key=lambda r: r[2][-1])
+    ref_err = float(best[2][-1])
+    ref_obj = fp64.aligned_error(best[0], truth)
+    problem = qpc.make_problem(intensity, support=support, mask=mask)
+    out = {"oracle": {"best_final_error": ref_err, "aligned_object_error": ref_obj,
+                      "seconds": ref_seconds}}
+    for storage in STORAGES:
+        ours = gpu_runs(problem, recipe, starts, storage)
+        b = min(ours, key=lambda r: r.error)
+        obj = fp64.aligned_error(b.object, truth)
+        out[storage] = {"best_final_error": b.error, "aligned_object_error": obj,
+                        "final_error_diff": abs(b.error - ref_err),
+                        "object_error_diff": abs(obj - ref_obj)}
+    return out
+
+
+def square_64(full):
+    obj = workloads.square(64, seed=0)
+    intensity = workloads.simulate_intensity(obj)
+    support = qpc.autocorrelation_support(intensity)
+    return {"workload": "square 64x64, 8 starts, default_recipe, noiseless, autocorrelation support",
+            "prefix": prefix(intensity, support, None, Recipe(RAAR(20)), 8),
+            "whole_recipe": whole(intensity, support, None, default_recipe(), 8, obj)}
+
+
+def gaussians_256(full):
+    obj, intensity, mask = workloads.gaussians(256, seed=1000)
+    support = qpc.autocorrelation_support(intensity)
+    out = {"workload": "gaussians 256x256, 32 starts, repeat(10, RAAR(50,0.9), Shrinkwrap(0.3,1)), "
+                       "ER(200), Poisson 1e6, beamstop 8",
+           "prefix": prefix(intensity, support, mask, Recipe(RAAR(20, 0.9)), 32)}
+    if full:
+        out["whole_recipe"] = whole(intensity, support, mask, workloads.gaussians_recipe(), 32, obj)
+    return out
+
+
+def uneven(full):
+    batch = workloads.uneven_batch(count=64, seed=2000)
+    by_side = {}
+    for obj, intensity, mask in batch:
+        support = qpc.autocorrelation_support(intensity)
+        res = prefix(intensity, support, mask, Recipe(HIO(20)), 4)
+        side = str(obj.shape[0])
+        cur = by_side.setdefault(side, {s: {"max_rel_error_diff": 0.0, "max_object_rel_l2": 0.0,
+                                            "problems": 0} for s in STORAGES})
+        for s in STORAGES:
+            for k in ("max_rel_error_diff", "max_object_rel_l2"):
+                cur[s][k] = max(cur[s][k], res["storage"][s][k])
+            cur[s]["problems"] += 1
+    return {"workload": "uneven batch, 64 problems, sides {64,128,256,512}, 4 starts; "
+                        "per side the worst problem of HIO(20) from the same seeds",
+            "prefix_by_side": by_side}
+
+
+def adjoint_512(full):
+    import torch
+
+    rng = np.random.default_rng(4000)
+    obj = workloads.square(512, seed=4000)
+    intensity = workloads.poisson(workloads.simulate_intensity(obj), 1e7, rng)
+    mask = workloads.beamstop((512, 512), 12)
+    ref_p = fp64.make_problem(intensity, None, mask)
+    p = qpc.make_problem(intensity, mask=mask)
+    model = qad.AmplitudeModel(p)
+    x = (obj + 0.1 * (rng.standard_normal(obj.shape) + 1j * rng.standard_normal(obj.shape))
+         ).astype(np.complex64)
+    xt = torch.from_numpy(np.ascontiguousarray(np.fft.ifftshift(x))).cuda()[None]
+    loss, grad = qad._loss_and_grad(xt, model.signed, model.shape)
+    g = np.fft.fftshift(grad[0].cpu().numpy())
+    projected, _ = fp64.modulus_project(ref_p, x)
+    identity = 2.0 * (x.astype(np.complex128) - projected)
+    fft = fp64.Fft(2, backend="scipy", workers=WORKERS)
+    y = fft.forward(fp64.to_fft_order(x.astype(np.complex128)))
+    amp = fp64.to_fft_order(ref_p.amplitude).astype(np.float64)
+    usable = fp64.to_fft_order(ref_p.mask) == 0
+    ref_loss = float(np.sum(np.where(usable, (np.abs(y) - amp) ** 2, 0.0)))
+    return {"workload": "square 512x512 (box 192), Poisson 1e7, beamstop 12: amplitude loss and "
+                        "its gradient at a perturbed truth (FP32 amplitude)",
+            "loss_rel_diff": abs(float(loss[0].item()) - ref_loss) / ref_loss,
+            "gradient_rel_l2_vs_2(x-P_M x)": fp64.relative_diff(g, identity)}
+
+
+def crystal_128(full):
+    obj, intensity = workloads.crystal(128, seed=3000)
+    support = qpc.autocorrelation_support(intensity)
+    return {"workload": "crystal 128^3, Poisson 1e7, 4 starts",
+            "prefix": prefix(intensity, support, None, Recipe(HIO(10)), 4)}
+
+
+REPORTS = {"square": square_64, "gaussians": gaussians_256, "uneven": uneven,
+           "adjoint": adjoint_512, "crystal": crystal_128}
+
+
+def main(argv=None):
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--full", action="store_true", help="whole recipes for every workload")
+    parser.add_argument("--only", choices=sorted(REPORTS), action="append")
+    args = parser.parse_args(argv)
+    for name in args.only or REPORTS:
+        t0 = time.perf_counter()
+        line = {"report": name, **REPORTS[name](args.full)}
+        line["seconds"] = time.perf_counter() - t0
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
