@@ -129,30 +129,38 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
     them (same seed -> same starting objects). Stops after ``steps`` steps or
     ``seconds`` of wall time, whichever comes first. Returns one
     ``Reconstruction`` per start; ``errors`` holds the Fourier error
-    sqrt(L / energy) of every step, the projection solvers' error measure."""
+    sqrt(L / energy) of every step, the projection solvers' error measure.
+
+    Adam's step is absolute in the units of its parameters, and measured
+    intensities fix the object's scale (counts), so the parameters are the
+    object divided by the root-mean-square amplitude that a support of this
+    size needs to carry the measured energy: ``lr`` is a step relative to the
+    object's typical amplitude, whatever the photon count."""
     torch = _torch()
     with Solver(problem, starts=starts, seed=seed, init=init) as drawn:
         first = drawn.results()
     model = AmplitudeModel(problem, device)
     ndim = len(model.shape)
     x0 = np.stack([np.fft.ifftshift(r.object) for r in first]).astype(np.complex64)
-    x = torch.from_numpy(x0).to(device).requires_grad_(True)
+    inside = max(int(model.support.sum().item()), 1)
+    scale = float(np.sqrt(model.energy / inside)) or 1.0
+    u = torch.from_numpy(x0 / np.float32(scale)).to(device).requires_grad_(True)
     support = model.support.to(torch.complex64)
-    opt = torch.optim.Adam([x], lr=lr)
+    opt = torch.optim.Adam([u], lr=lr)
     history = []
     t0 = time.perf_counter()
     for _ in range(steps):
         opt.zero_grad(set_to_none=True)
-        losses = amplitude_loss(x, model)
+        losses = amplitude_loss(u * scale, model)
         losses.sum().backward()
         history.append(losses.detach())
         opt.step()
         with torch.no_grad():
-            x.mul_(support)
+            u.mul_(support)
         if seconds is not None and time.perf_counter() - t0 >= seconds:
             break
     torch.cuda.synchronize()
     errors = torch.sqrt(torch.stack(history) / (model.energy + 1e-12)).to(torch.float32).cpu().numpy()
-    final = to_centred(x.detach(), ndim).cpu().numpy()
+    final = to_centred(u.detach() * scale, ndim).cpu().numpy()
     supp = np.fft.fftshift(model.support.cpu().numpy(), axes=tuple(range(-ndim, 0)))
     return [Reconstruction(final[s], supp.copy(), errors[:, s].copy()) for s in range(starts)]

@@ -5,15 +5,17 @@ JSON line per workload.
 
     python tests/precision_report.py [--full] [--only NAME ...]
 
-For each workload and storage: a prefix of iterations from the same seeds
-(the random starts are bit-identical by construction) compared start by start
-with the oracle -- the largest relative difference of the per-iteration
-Fourier errors and the relative L2 difference of the objects -- and, where
-the oracle finishes in about a minute (or everywhere with --full), the whole
-recipe: the best start's final Fourier error and its object error against the
-ground truth after phase-ramp and twin alignment, each beside the oracle's.
-Iterative recipes are chaotic (long runs from one start diverge at rounding
-level), so whole recipes are compared through those two numbers.
+For each workload and storage: prefixes of 2 and 10-20 iterations from the
+same seeds (the random starts are bit-identical by construction) compared
+start by start with the oracle -- the largest relative difference of the
+per-iteration Fourier errors and the relative L2 difference of the objects --
+and, where the oracle finishes in about a minute (or everywhere with --full),
+the whole recipe: the best start's final Fourier error and its object error
+against the ground truth (scaled to the data) after phase-ramp and twin
+alignment. Every comparison is repeated for the oracle's own FP32 port
+(complex64 numpy): iterative recipes are chaotic, and on some problems
+rounding alone moves an HIO or RAAR run by order one within 20 iterations;
+the port's numbers show how far it carries each recipe on each problem.
 """
 
 from __future__ import annotations
@@ -42,9 +44,10 @@ STORAGES = ("f32", "f16", "bf16")
 WORKERS = len(os.sched_getaffinity(0))
 
 
-def oracle_runs(intensity, support, mask, ops, starts, seed=0):
+def oracle_runs(intensity, support, mask, ops, starts, seed=0, dtype=np.complex128):
     problem = fp64.make_problem(intensity, support, mask)
-    solver = fp64.Solver(problem, starts=starts, seed=seed, fft="scipy", workers=WORKERS)
+    solver = fp64.Solver(problem, starts=starts, seed=seed, fft="scipy", workers=WORKERS,
+                         dtype=dtype)
     solver.run(ops)
     return solver.results()
 
@@ -55,38 +58,63 @@ def gpu_runs(problem, recipe, starts, storage, seed=0):
         return s.results()
 
 
+def diffs(runs, ref):
+    """Largest relative difference of the error histories and of the objects."""
+    err = max(float(np.max(np.abs(np.asarray(r[2]) - e) / np.maximum(e, 1e-12)))
+              for (_, _, e), r in zip(ref, runs))
+    obj = max(fp64.relative_diff(r[0], o) for (o, _, _), r in zip(ref, runs))
+    return {"max_rel_error_diff": err, "max_object_rel_l2": obj}
+
+
 def prefix(intensity, support, mask, recipe, starts):
-    """Start-by-start comparison over a short recipe, per storage."""
+    """Start-by-start comparison over a short recipe, per storage, beside the
+    same comparison for the oracle's own FP32 port: how far rounding alone
+    carries this recipe on this problem."""
     ref = oracle_runs(intensity, support, mask, recipe.ops(), starts)
+    port = oracle_runs(intensity, support, mask, recipe.ops(), starts, dtype=np.complex64)
     problem = qpc.make_problem(intensity, support=support, mask=mask)
-    out = {}
+    out = {"fp32_port": diffs(port, ref)}
     for storage in STORAGES:
-        ours = gpu_runs(problem, recipe, starts, storage)
-        err = max(float(np.max(np.abs(r.errors - e) / np.maximum(e, 1e-12)))
-                  for (_, _, e), r in zip(ref, ours))
-        obj = max(fp64.relative_diff(r.object, o) for (o, _, _), r in zip(ref, ours))
-        out[storage] = {"max_rel_error_diff": err, "max_object_rel_l2": obj}
+        ours = [(r.object, r.support, r.errors) for r in gpu_runs(problem, recipe, starts, storage)]
+        out[storage] = diffs(ours, ref)
     return {"recipe": repr(recipe.ops()), "starts": starts, "storage": out}
 
 
+def prefixes(intensity, support, mask, kind, starts, lengths=(2, 20)):
+    ops = {"raar": lambda n: Recipe(RAAR(n, 0.9)), "hio": lambda n: Recipe(HIO(n))}[kind]
+    return {str(n): prefix(intensity, support, mask, ops(n), starts) for n in lengths}
+
+
+def scaled_truth(truth, intensity):
+    """The ground truth at the data's scale (Parseval with the unitary FFT)."""
+    scale = np.sqrt(float(np.sum(intensity, dtype=np.float64)) /
+                    float(np.sum(np.abs(truth.astype(np.complex128)) ** 2)))
+    return truth * scale
+
+
 def whole(intensity, support, mask, recipe, starts, truth):
-    """Best start's final error and aligned object error, ours beside the oracle's."""
-    t0 = time.perf_counter()
-    ref = oracle_runs(intensity, support, mask, recipe.ops(), starts)
-    ref_seconds = time.perf_counter() - t0
-    best = min(ref, key=lambda r: r[2][-1])
-    ref_err = float(best[2][-1])
-    ref_obj = fp64.aligned_error(best[0], truth)
+    """Best start's final error and aligned object error for ours, the FP64
+    oracle and its FP32 port."""
+    truth = scaled_truth(truth, intensity)
+    out = {}
+    ref_err = ref_obj = None
+    for name, dtype in (("oracle_fp64", np.complex128), ("fp32_port", np.complex64)):
+        t0 = time.perf_counter()
+        runs = oracle_runs(intensity, support, mask, recipe.ops(), starts, dtype=dtype)
+        best = min(runs, key=lambda r: r[2][-1])
+        err, obj = float(best[2][-1]), fp64.aligned_error(best[0], truth)
+        if ref_err is None:
+            ref_err, ref_obj = err, obj
+        out[name] = {"best_final_error": err, "aligned_object_error": obj,
+                     "seconds": time.perf_counter() - t0}
     problem = qpc.make_problem(intensity, support=support, mask=mask)
-    out = {"oracle": {"best_final_error": ref_err, "aligned_object_error": ref_obj,
-                      "seconds": ref_seconds}}
     for storage in STORAGES:
-        ours = gpu_runs(problem, recipe, starts, storage)
-        b = min(ours, key=lambda r: r.error)
-        obj = fp64.aligned_error(b.object, truth)
-        out[storage] = {"best_final_error": b.error, "aligned_object_error": obj,
-                        "final_error_diff": abs(b.error - ref_err),
-                        "object_error_diff": abs(obj - ref_obj)}
+        b = min(gpu_runs(problem, recipe, starts, storage), key=lambda r: r.error)
+        out[storage] = {"best_final_error": b.error,
+                        "aligned_object_error": fp64.aligned_error(b.object, truth)}
+    for v in out.values():
+        v["final_error_diff"] = abs(v["best_final_error"] - ref_err)
+        v["object_error_diff"] = abs(v["aligned_object_error"] - ref_obj)
     return out
 
 
@@ -95,7 +123,7 @@ def square_64(full):
     intensity = workloads.simulate_intensity(obj)
     support = qpc.autocorrelation_support(intensity)
     return {"workload": "square 64x64, 8 starts, default_recipe, noiseless, autocorrelation support",
-            "prefix": prefix(intensity, support, None, Recipe(RAAR(20)), 8),
+            "prefix": prefixes(intensity, support, None, "raar", 8),
             "whole_recipe": whole(intensity, support, None, default_recipe(), 8, obj)}
 
 
@@ -104,7 +132,7 @@ def gaussians_256(full):
     support = qpc.autocorrelation_support(intensity)
     out = {"workload": "gaussians 256x256, 32 starts, repeat(10, RAAR(50,0.9), Shrinkwrap(0.3,1)), "
                        "ER(200), Poisson 1e6, beamstop 8",
-           "prefix": prefix(intensity, support, mask, Recipe(RAAR(20, 0.9)), 32)}
+           "prefix": prefixes(intensity, support, mask, "raar", 32)}
     if full:
         out["whole_recipe"] = whole(intensity, support, mask, workloads.gaussians_recipe(), 32, obj)
     return out
@@ -113,18 +141,20 @@ def gaussians_256(full):
 def uneven(full):
     batch = workloads.uneven_batch(count=64, seed=2000)
     by_side = {}
+    names = ("fp32_port",) + STORAGES
     for obj, intensity, mask in batch:
         support = qpc.autocorrelation_support(intensity)
-        res = prefix(intensity, support, mask, Recipe(HIO(20)), 4)
-        side = str(obj.shape[0])
-        cur = by_side.setdefault(side, {s: {"max_rel_error_diff": 0.0, "max_object_rel_l2": 0.0,
-                                            "problems": 0} for s in STORAGES})
-        for s in STORAGES:
-            for k in ("max_rel_error_diff", "max_object_rel_l2"):
-                cur[s][k] = max(cur[s][k], res["storage"][s][k])
-            cur[s]["problems"] += 1
-    return {"workload": "uneven batch, 64 problems, sides {64,128,256,512}, 4 starts; "
-                        "per side the worst problem of HIO(20) from the same seeds",
+        res = prefixes(intensity, support, mask, "hio", 4)
+        side = by_side.setdefault(str(obj.shape[0]), {"problems": 0})
+        side["problems"] += 1
+        for n, r in res.items():
+            cur = side.setdefault(n, {k: {"max_rel_error_diff": 0.0, "max_object_rel_l2": 0.0}
+                                      for k in names})
+            for k in names:
+                for m in ("max_rel_error_diff", "max_object_rel_l2"):
+                    cur[k][m] = max(cur[k][m], r["storage"][k][m])
+    return {"workload": "uneven batch, 64 problems, sides {64,128,256,512}, 4 starts; per side "
+                        "and prefix length (HIO iterations) the worst problem, from the same seeds",
             "prefix_by_side": by_side}
 
 
@@ -160,7 +190,7 @@ def crystal_128(full):
     obj, intensity = workloads.crystal(128, seed=3000)
     support = qpc.autocorrelation_support(intensity)
     return {"workload": "crystal 128^3, Poisson 1e7, 4 starts",
-            "prefix": prefix(intensity, support, None, Recipe(HIO(10)), 4)}
+            "prefix": prefixes(intensity, support, None, "hio", 4, lengths=(2, 10))}
 
 
 REPORTS = {"square": square_64, "gaussians": gaussians_256, "uneven": uneven,
