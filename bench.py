@@ -226,15 +226,19 @@ def run_profile(iterations, schedule="streamed"):
     return 0
 
 
-def run_profile_step(sync_every):
-    """One benchmark step (the whole recipe over 32 starts, tuned schedule)
-    after the solver is built, for an ncu launch list of the timed work."""
+def run_profile_step(sync_every, batch=0, schedule="auto"):
+    """One benchmark step (the whole recipe over 32 starts) after the solver is
+    built, for an ncu launch list of the timed work. The autotuner times its
+    candidates by wall clock, which a profiler distorts, so a launch list is
+    taken with the schedule fixed (--batch/--schedule) to the one a plain run
+    picks."""
     import qoraphasecu_b200 as qpc
     from qoraphasecu_b200 import workloads
 
     _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
     problem = qpc.make_problem(intensity, mask=mask)
-    with qpc.Solver(problem, starts=STARTS, seed=0, sync_every=sync_every) as solver:
+    with qpc.Solver(problem, starts=STARTS, seed=0, sync_every=sync_every, batch=batch or None,
+                    schedule=schedule) as solver:
         before = qpc.kernel_launches()
         solver.run(workloads.gaussians_recipe())
         print(json.dumps({"step_kernels": qpc.kernel_launches() - before,
@@ -422,7 +426,7 @@ def main(argv=None):
     if args.profile:
         return run_profile(args.profile, "resident" if args.schedule == "resident" else "streamed")
     if args.profile_step:
-        return run_profile_step(args.sync_every)
+        return run_profile_step(args.sync_every, args.batch, args.schedule)
     if args.workload:
         print(json.dumps({"workload_report": args.workload, **WORKLOADS[args.workload](args)}))
         return 0

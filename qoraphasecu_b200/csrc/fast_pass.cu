@@ -35,7 +35,7 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 // and, for row passes that move whole tiles by bulk copies, the wave tile in
 // and out (its rows are contiguous in global memory); then the side inputs
 // staged by bulk copies (the amplitude tile of a modulus pass; the old-iterate
-// and support tiles of a row update); then the mbarrier.
+// and support tiles of a row update); then two mbarriers (16 bytes).
 template <int L, bool ROWS, Mode M, class AmpT>
 struct Staging {
   using G = Geometry<L>;
@@ -116,11 +116,21 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
   // update. They hold no registers while in flight.
   unsigned char* sbase = reinterpret_cast<unsigned char*>(smem);
   [[maybe_unused]] float2* wtile = smem;  // region W, rows of length L (bulk-copied passes)
+  // Two barriers: `bar` for the input tile (or the amplitude), `side_bar` for
+  // the old iterate and support of a row update, which are needed only after
+  // the inverse transform, so their copies overlap it.
   [[maybe_unused]] auto* bar = reinterpret_cast<std::uint64_t*>(sbase + St::kBarrier);
+  [[maybe_unused]] std::uint64_t* side_bar = St::kUpd ? bar + 1 : bar;
   if constexpr (St::kBarrierUsed) {
     if (tid == 0) {
       mbar_init(bar, 1);
-      mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTile : 0) + St::kSideA + St::kSideB);
+      if constexpr (St::kUpd) {
+        mbar_arrive_expect_tx(bar, St::kTile);
+        mbar_init(side_bar, 1);
+        mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSideB);
+      } else {
+        mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTile : 0) + St::kSideA + St::kSideB);
+      }
     }
     __syncthreads();
     if constexpr (St::kRowTma) {
@@ -131,8 +141,8 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
     }
     if constexpr (St::kUpd) {
       if (tid == 0) {
-        bulk_g2s(sbase + St::kExchange, p.x + line0 * L, St::kSideA, bar);
-        bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, bar);
+        bulk_g2s(sbase + St::kExchange, p.x + line0 * L, St::kSideA, side_bar);
+        bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, side_bar);
       }
     } else if constexpr (St::kAmp) {
       if (ROWS || p.amp_tiled) {
@@ -161,8 +171,8 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
 
   // Every thread waits (bounded); if any gave up, the CTA records it and
   // leaves together, writing nothing.
-  auto staged = [&]() -> bool {
-    if (!__syncthreads_and(mbar_wait(bar, 0) ? 1 : 0)) {
+  auto staged = [&](std::uint64_t* b) -> bool {
+    if (!__syncthreads_and(mbar_wait(b, 0) ? 1 : 0)) {
       if (tid == 0) atomicAdd(&g_fast_wait_failures, 1);
       return false;
     }
@@ -171,7 +181,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
 
   float2 v[E];
   if constexpr (St::kRowTma) {
-    if (!staged()) return;
+    if (!staged(bar)) return;
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = wtile[l * L + t + T * m];
     __syncthreads();  // region W becomes the exchange buffer
@@ -193,7 +203,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
   transform<L, kStartsInverse, kWarpLocal>(v, t, tw, row);
 
   if constexpr (St::kAmp) {
-    if (!staged()) return;
+    if (!staged(bar)) return;
   }
 
   if constexpr (M == Mode::kMod || M == Mode::kGrad) {
@@ -211,6 +221,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
     transform<L, true, kWarpLocal>(v, t, tw, row);
   } else if constexpr (M == Mode::kUpd) {
     if constexpr (St::kUpd) {
+      if (!staged(side_bar)) return;
       // x_new replaces the old iterate in its tile and leaves by one bulk store.
       float2* x_tile = reinterpret_cast<float2*>(sbase + St::kExchange);
       const std::uint8_t* s_tile = sbase + St::kExchange + St::kSideA;
