@@ -459,19 +459,16 @@ def main(argv=None):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v: float) -> float:
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from qoraphasecu_b200.replicas import max_over_ranks, rank_seed
+
+    seed = rank_seed(0, rank)  # replicas draw distinct random starts
 
     _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
     recipe = workloads.gaussians_recipe()
     iters = recipe.iterations()
     stream = torch.cuda.current_stream()
     problem = qpc.make_problem(intensity, mask=mask)
-    solver = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+    solver = qpc.Solver(problem, starts=STARTS, seed=seed, sync_every=args.sync_every,
                         batch=args.batch or None, device=local, stream=stream.cuda_stream,
                         schedule=args.schedule)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
@@ -501,7 +498,7 @@ def main(argv=None):
 
     # Per-kernel device time: every pass of an iteration launched directly
     # between CUDA events on the same stream, all 32 starts in one launch.
-    with qpc.Solver(problem, starts=STARTS, seed=rank, batch=STARTS, device=local,
+    with qpc.Solver(problem, starts=STARTS, seed=seed, batch=STARTS, device=local,
                     stream=stream.cuda_stream) as single:
         single.run(workloads.hio_recipe(5))
         pass_ms = single.profile_passes(20)
@@ -571,7 +568,7 @@ def main(argv=None):
 
     if not args.no_extras:
         # Plain per-start path (the in-repo baseline), one step.
-        plain = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+        plain = qpc.Solver(problem, starts=STARTS, seed=seed, sync_every=args.sync_every,
                            variant="plain", device=local, stream=stream.cuda_stream)
         plain.run(recipe)
         barrier()
@@ -585,7 +582,7 @@ def main(argv=None):
         plain.close()
         plain_value = world * STARTS * iters / (plain_ms / 1e3)
         # FP16 amplitude storage, same schedule.
-        half = qpc.Solver(problem, starts=STARTS, seed=rank, sync_every=args.sync_every,
+        half = qpc.Solver(problem, starts=STARTS, seed=seed, sync_every=args.sync_every,
                           amp_storage="f16", device=local, stream=stream.cuda_stream)
         half.run(recipe)
         barrier()
@@ -610,7 +607,7 @@ def main(argv=None):
         for k in range(args.warmup + args.steps):
             barrier()
             t0 = time.perf_counter()
-            ens = qpc.reconstruct(host_in, mask=mask, recipe=recipe, starts=STARTS, seed=rank,
+            ens = qpc.reconstruct(host_in, mask=mask, recipe=recipe, starts=STARTS, seed=seed,
                                   sync_every=args.sync_every)
             times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(statistics.median(times[args.warmup:]))
