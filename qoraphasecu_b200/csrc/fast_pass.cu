@@ -36,9 +36,24 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 // and out (its rows are contiguous in global memory); then the side inputs
 // staged by bulk copies (the amplitude tile of a modulus pass; the old-iterate
 // and support tiles of a row update); then two mbarriers (16 bytes).
+// CTA shape of a streamed pass: lines per CTA, threads, the CTAs per SM the
+// register budget is sized for (registers <= 64K / (NT * MIN_CTAS)) and the
+// exchange rows. Rows of 256 points use 8 lines per CTA (128 threads, up to 6
+// CTAs per SM), which halves a launch's last partial wave; their columns keep
+// 16, whose 128-byte row segments load better.
+template <int L, bool ROWS>
+struct Tiling {
+  using G = Geometry<L>;
+  static constexpr int LINES =
+      (ROWS && L == 256) ? 8 : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
+  static constexpr int NT = G::T * LINES;
+  static constexpr int MIN_CTAS = NT <= 128 ? 6 : (NT <= 256 ? 3 : 1);
+  static constexpr int SMEM = G::STAGES > 1 ? LINES * G::PITCH * 8 : 0;
+};
+
 template <int L, bool ROWS, Mode M, class AmpT>
 struct Staging {
-  using G = Geometry<L>;
+  using G = Tiling<L, ROWS>;
   static constexpr int kTile = G::LINES * L * 8;  // one complex64 tile
   static constexpr bool kRowTma =
       ROWS && (M == Mode::kFwd || M == Mode::kFwdFromX || M == Mode::kInv || M == Mode::kUpd);
@@ -56,18 +71,20 @@ struct Staging {
 };
 
 template <int L, bool ROWS, Mode M, class AmpT>
-__global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_pass_kernel(const PassParams p) {
+__global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS)
+    fast_pass_kernel(const PassParams p) {
   using G = Geometry<L>;
+  using Ti = Tiling<L, ROWS>;
   using St = Staging<L, ROWS, M, AmpT>;
   constexpr int E = G::E;
   constexpr int T = G::T;
   extern __shared__ float2 smem[];
   const int tid = threadIdx.x;
-  const int l = ROWS ? tid / T : tid % G::LINES;
-  const int t = ROWS ? tid % T : tid / G::LINES;
+  const int l = ROWS ? tid / T : tid % Ti::LINES;
+  const int t = ROWS ? tid % T : tid / Ti::LINES;
   float2* row = smem + l * G::PITCH;
 
-  const long long line0 = static_cast<long long>(blockIdx.x) * G::LINES;
+  const long long line0 = static_cast<long long>(blockIdx.x) * Ti::LINES;
   const int batch_start = static_cast<int>(line0 / p.lines_per_start);
   const long long start_off = static_cast<long long>(batch_start) * p.n;
   // Element t + T m of line (line0 + l) sits at base + (t + T m) * S; the
@@ -160,8 +177,8 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
         const long long outer = line0 / p.S;
         const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
                           (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
-        constexpr int kRowBytes = G::LINES * static_cast<int>(sizeof(AmpT));
-        for (int j = tid; j < L; j += G::NT) {
+        constexpr int kRowBytes = Ti::LINES * static_cast<int>(sizeof(AmpT));
+        for (int j = tid; j < L; j += Ti::NT) {
           bulk_g2s(sbase + St::kExchange + j * kRowBytes, src + static_cast<long long>(j) * p.S,
                    kRowBytes, bar);
         }
@@ -213,7 +230,7 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const int j = t + T * m;
-      const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * G::LINES + l]);
+      const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * Ti::LINES + l]);
       v[m] = pointwise_projection<M>(v[m], a, s, acc);
     }
     const double total = block_sum_double(static_cast<double>(acc));
@@ -318,10 +335,10 @@ __global__ void __launch_bounds__(Geometry<L>::NT, Geometry<L>::MIN_CTAS) fast_p
 
 template <int L, bool ROWS, Mode M, class AmpT>
 void launch_one(const PassParams& p, cudaStream_t stream) {
-  using G = Geometry<L>;
-  const dim3 grid(static_cast<unsigned>(p.lines / G::LINES));
+  using Ti = Tiling<L, ROWS>;
+  const dim3 grid(static_cast<unsigned>(p.lines / Ti::LINES));
   fast_pass_kernel<L, ROWS, M, AmpT>
-      <<<grid, G::NT, Staging<L, ROWS, M, AmpT>::kBytes, stream>>>(p);
+      <<<grid, Ti::NT, Staging<L, ROWS, M, AmpT>::kBytes, stream>>>(p);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }
@@ -374,19 +391,19 @@ void launch_length(Mode mode, const PassParams& p, cudaStream_t stream) {
 }
 
 template <int L>
-int lines_per_cta() {
-  return Geometry<L>::LINES;
+int lines_per_cta(bool rows) {
+  return rows ? Tiling<L, true>::LINES : Tiling<L, false>::LINES;
 }
 
-int fast_lines(int L) {
+int fast_lines(int L, bool rows) {
   switch (L) {
-    case 16: return lines_per_cta<16>();
-    case 32: return lines_per_cta<32>();
-    case 64: return lines_per_cta<64>();
-    case 128: return lines_per_cta<128>();
-    case 256: return lines_per_cta<256>();
-    case 512: return lines_per_cta<512>();
-    case 1024: return lines_per_cta<1024>();
+    case 16: return lines_per_cta<16>(rows);
+    case 32: return lines_per_cta<32>(rows);
+    case 64: return lines_per_cta<64>(rows);
+    case 128: return lines_per_cta<128>(rows);
+    case 256: return lines_per_cta<256>(rows);
+    case 512: return lines_per_cta<512>(rows);
+    case 1024: return lines_per_cta<1024>(rows);
     default: return 0;
   }
 }
@@ -449,7 +466,7 @@ bool fast_passes_enabled() {
 }
 
 int fast_pass_lines(const PassParams& p) {
-  return fast_passes_enabled() && fast_pass_supports(p) ? fast_lines(p.L) : 0;
+  return fast_passes_enabled() && fast_pass_supports(p) ? fast_lines(p.L, p.S == 1) : 0;
 }
 
 std::vector<unsigned char> tile_amplitude(const std::vector<unsigned char>& amp,
@@ -482,7 +499,7 @@ int take_fast_wait_failures() {
 }
 
 bool fast_pass_supports(const PassParams& p) {
-  const int lines = fast_lines(p.L);
+  const int lines = fast_lines(p.L, p.S == 1);
   if (lines == 0) return false;
   if (p.lines_per_start % lines != 0 || p.lines % lines != 0) return false;
   // Columns: the CTA's lines must be adjacent within one outer slab.

@@ -26,17 +26,12 @@ template <int L>
 struct Geometry {
   static constexpr int E = L == 32 || L == 64 ? 8 : 16;
   static constexpr int T = L / E;
-  static constexpr int LINES = T <= 16 ? 256 / T : (L >= 1024 ? 8 : 16);
-  static constexpr int NT = T * LINES;
-  // CTAs per SM the register budget is sized for (registers <= 64K / (NT * MIN_CTAS)).
-  static constexpr int MIN_CTAS = NT <= 256 ? 3 : 1;
   // Radix of each stage (product = L, each <= E).
   static constexpr int R0 = L <= 16 ? L : E;
   static constexpr int R1 = L <= 16 ? 1 : (L / R0 <= E ? L / R0 : E);
   static constexpr int R2 = L / (R0 * R1);
   static constexpr int STAGES = L <= 16 ? 1 : (R2 == 1 ? 2 : 3);
   static constexpr int PITCH = swz(L) + 1;
-  static constexpr int SMEM = STAGES > 1 ? LINES * PITCH * 8 : 0;
   static_assert(R0 * R1 * R2 == L, "bad factorisation");
   static_assert(R2 <= E && R1 <= E, "radix above the register count");
 };
