@@ -231,6 +231,20 @@ QPB_API qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int b
                                            const float* signed_amplitude, const float* x,
                                            float* grad, double* loss, void* stream);
 
+/* qpcu::aligned_error (include/qoraphasecu/metrics.hpp:12, src/core/metrics.cpp:17-86)
+ * for `batch` candidates at once, on the device: out[b] = ||a_b - ref|| / ||ref||
+ * after the best integer translation (cross-correlation peak), global phase and
+ * twin (conj(a(-r))). a: batch * numel complex64, reference: numel complex64,
+ * out: batch floats; host arrays. */
+QPB_API qpb_status qpb_aligned_error(const float* a, const float* reference, int ndim,
+                                     const int64_t* shape, int batch, float* out);
+
+/* qpcu::simulate_intensity (problem.hpp:42, problem.cpp:90-99): |centred unitary
+ * FFT(object)|^2 of a centre-origin complex64 object, the transform on the
+ * device. Host arrays of numel elements. */
+QPB_API qpb_status qpb_simulate_intensity(const float* object, int ndim, const int64_t* shape,
+                                          float* out);
+
 /* Single operators on centre-origin arrays (qpcu::cuda::, operators.hpp:25-33). */
 QPB_API qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
                                float* error_out);

@@ -17,6 +17,7 @@ from .api import (
     Problem,
     Reconstruction,
     Solver,
+    aligned_error,
     autocorrelation_support,
     best_index,
     cuda_available,
@@ -26,6 +27,7 @@ from .api import (
     reconstruct,
     reconstruct_batch,
     set_device,
+    simulate_intensity,
 )
 from .operators import gaussian_blur, modulus_project, support_project
 from .recipe import ER, HIO, RAAR, Recipe, Shrinkwrap, default_recipe, detwin, repeat
@@ -41,6 +43,7 @@ __all__ = [
     "Reconstruction",
     "Shrinkwrap",
     "Solver",
+    "aligned_error",
     "autocorrelation_support",
     "best_index",
     "cuda_available",
@@ -53,5 +56,6 @@ __all__ = [
     "reconstruct",
     "reconstruct_batch",
     "repeat",
+    "simulate_intensity",
     "support_project",
 ]

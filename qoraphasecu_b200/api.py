@@ -129,6 +129,33 @@ def half_support(support, axis: int = 0) -> np.ndarray:
     return out.astype(bool)
 
 
+def aligned_error(a, reference):
+    """``||a - reference|| / ||reference||`` after removing shift, global phase
+    and twin (python/qoraphasecu/api.py:89-95 of the reference), on the device.
+    ``a`` may also be a stack ``(batch, *reference.shape)``: then one error per
+    object comes back, computed in one batch."""
+    a = np.ascontiguousarray(a, dtype=np.complex64)
+    reference = np.ascontiguousarray(reference, dtype=np.complex64)
+    stacked = a.ndim == reference.ndim + 1 and a.shape[1:] == reference.shape
+    if a.shape != reference.shape and not stacked:
+        raise ValueError(f"shapes differ: {a.shape} vs {reference.shape}")
+    batch = a.shape[0] if stacked else 1
+    out = np.empty(batch, np.float32)
+    _lib.check(_lib.load().qpb_aligned_error(_lib.ptr(a), _lib.ptr(reference), reference.ndim,
+                                             _shape(reference), batch, _lib.ptr(out)))
+    return out if stacked else float(out[0])
+
+
+def simulate_intensity(obj) -> np.ndarray:
+    """|centred unitary FFT(obj)|^2 as float32 (src/core/problem.cpp:90-99), the
+    transform on the device."""
+    obj = np.ascontiguousarray(obj, dtype=np.complex64)
+    out = np.empty(obj.shape, np.float32)
+    _lib.check(_lib.load().qpb_simulate_intensity(_lib.ptr(obj), obj.ndim, _shape(obj),
+                                                  _lib.ptr(out)))
+    return out
+
+
 @dataclass
 class Problem:
     """Centre-origin amplitude, mask and support (the reference's qpcu::Problem)."""
@@ -508,6 +535,7 @@ __all__ = [
     "Recipe",
     "Reconstruction",
     "Solver",
+    "aligned_error",
     "autocorrelation_support",
     "best_index",
     "cuda_available",
@@ -515,4 +543,5 @@ __all__ = [
     "make_problem",
     "reconstruct",
     "reconstruct_batch",
+    "simulate_intensity",
 ]

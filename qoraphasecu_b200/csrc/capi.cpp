@@ -320,6 +320,30 @@ void qpb_destroy(qpb_solver* solver) {
   delete solver;
 }
 
+qpb_status qpb_aligned_error(const float* a, const float* reference, int ndim,
+                             const int64_t* shape, int batch, float* out) {
+  return guarded([&] {
+    require(a && reference && out, "NULL array");
+    numel_checked(ndim, shape);
+    require(batch >= 1, "batch must be >= 1");
+    long long sh[3] = {0, 0, 0};
+    for (int k = 0; k < ndim; ++k) sh[k] = shape[k];
+    qpb::aligned_error(reinterpret_cast<const float2*>(a), reinterpret_cast<const float2*>(reference),
+                       ndim, sh, batch, out);
+  });
+}
+
+qpb_status qpb_simulate_intensity(const float* object, int ndim, const int64_t* shape,
+                                  float* out) {
+  return guarded([&] {
+    require(object && out, "NULL array");
+    numel_checked(ndim, shape);
+    long long sh[3] = {0, 0, 0};
+    for (int k = 0; k < ndim; ++k) sh[k] = shape[k];
+    qpb::simulate_intensity(reinterpret_cast<const float2*>(object), ndim, sh, out);
+  });
+}
+
 qpb_status qpb_modulus_project(const qpb_problem* problem, float* obj, int amp_storage,
                                float* error_out) {
   return guarded([&] {

@@ -310,6 +310,14 @@ void gaussian_blur(const float* image, int ndim, const long long* shape, float s
 // Loose support: |IFFT(intensity)| > threshold * max, centre-origin (problem.cpp:72-88).
 void autocorrelation_support(const float* intensity, int ndim, const long long* shape,
                              float threshold, std::uint8_t* out);
+// aligned_error (metrics.cpp:17-86) of `batch` candidates a[b] (numel complex64
+// each) against one reference, on the device; out[b] = the smaller of the
+// direct and twin errors. Host arrays.
+void aligned_error(const float2* a, const float2* reference, int ndim, const long long* shape,
+                   int batch, float* out);
+// simulate_intensity (problem.cpp:90-99): |centred unitary FFT(object)|^2 of a
+// centre-origin complex64 object, FFT on the device. Host arrays.
+void simulate_intensity(const float2* object, int ndim, const long long* shape, float* out);
 // half_support on the device (problem.cpp:101-127), centre-origin in and out.
 void half_support(const std::uint8_t* support, int ndim, const long long* shape, int axis,
                   std::uint8_t* out);

@@ -97,6 +97,23 @@ def test_create_batch_validates_before_touching_a_device():
     assert handle.value is None
 
 
+def test_metrics_validate_before_touching_a_device():
+    lib = _lib.load()
+    a = np.zeros((4, 4), np.complex64)
+    out = np.zeros(1, np.float32)
+    shape = _lib.shape_arg((4, 4))
+    assert lib.qpb_aligned_error(_lib.ptr(a), None, 2, shape, 1, _lib.ptr(out)) == \
+        _lib.INVALID_ARGUMENT
+    assert lib.qpb_aligned_error(_lib.ptr(a), _lib.ptr(a), 4, shape, 1, _lib.ptr(out)) == \
+        _lib.INVALID_ARGUMENT
+    assert lib.qpb_aligned_error(_lib.ptr(a), _lib.ptr(a), 2, shape, 0, _lib.ptr(out)) == \
+        _lib.INVALID_ARGUMENT
+    assert lib.qpb_simulate_intensity(_lib.ptr(a), 1, shape, _lib.ptr(out)) == \
+        _lib.INVALID_ARGUMENT
+    with pytest.raises(ValueError, match="shapes differ"):
+        qpc.aligned_error(a, np.zeros((4, 5), np.complex64))
+
+
 def test_run_rejects_null_solver_and_bad_recipes():
     lib = _lib.load()
     ops = (_lib.Op * 1)(_lib.Op(0, 0, 0, 0, 0, 0, 0))
