@@ -141,6 +141,30 @@ QPB_API qpb_status qpb_half_support(const uint8_t* support, int ndim, const int6
  * the starts. */
 QPB_API qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qpb_solver** out);
 
+/* Device-resident inputs and outputs (no counterpart in the reference, whose
+ * Python layer copies through numpy, python/bindings.cpp:37-41): callers that
+ * hold their data in device memory (torch tensors, a detector pipeline's
+ * buffers) set up, run and read a reconstruction without any array crossing to
+ * the host.
+ *   qpb_make_problem_device: qpb_make_problem on device arrays (centre-origin,
+ * numel each; support and mask may be NULL), the autocorrelation support
+ * computed on the device; enqueued on `stream` (a cudaStream_t, NULL = legacy
+ * default stream), returns after it completes.
+ *   qpb_create_device: qpb_create whose problem arrays are device pointers;
+ * options->start, when given, is a device pointer too.
+ *   qpb_results_device: qpb_results with objects (starts * numel complex64) and
+ * supports (starts * numel) written to device memory; errors to host memory.
+ * Problems of one shape only. */
+QPB_API qpb_status qpb_make_problem_device(const float* intensity, int ndim, const int64_t* shape,
+                                           const uint8_t* support, const uint8_t* mask,
+                                           float support_threshold, float* amplitude_out,
+                                           uint8_t* mask_out, uint8_t* support_out,
+                                           void* stream);
+QPB_API qpb_status qpb_create_device(const qpb_problem* problem, const qpb_options* options,
+                                     qpb_solver** out);
+QPB_API qpb_status qpb_results_device(qpb_solver* solver, float* objects, uint8_t* supports,
+                                      float* errors);
+
 /* Many problems, any mix of shapes, reconstructed together (no counterpart in
  * the reference, which builds one solver per problem). options->starts starts
  * per problem; options->start, when given, holds every problem's starts in

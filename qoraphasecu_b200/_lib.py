@@ -45,6 +45,9 @@ EXPORTS = (
     "qpb_half_support",
     "qpb_create",
     "qpb_create_batch",
+    "qpb_make_problem_device",
+    "qpb_create_device",
+    "qpb_results_device",
     "qpb_run",
     "qpb_set_progress",
     "qpb_error_count",
@@ -137,6 +140,11 @@ def load():
         lib.qpb_create.argtypes = [POINTER(Problem), POINTER(Options), POINTER(c_void_p)]
         lib.qpb_create_batch.argtypes = [POINTER(Problem), c_size_t, POINTER(Options),
                                          POINTER(c_void_p)]
+        lib.qpb_make_problem_device.argtypes = [c_void_p, c_int, POINTER(c_int64), c_void_p,
+                                                c_void_p, c_float, c_void_p, c_void_p, c_void_p,
+                                                c_void_p]
+        lib.qpb_create_device.argtypes = [POINTER(Problem), POINTER(Options), POINTER(c_void_p)]
+        lib.qpb_results_device.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_run.argtypes = [c_void_p, POINTER(Op), c_size_t]
         lib.qpb_set_progress.argtypes = [c_void_p, PROGRESS, c_void_p]
         lib.qpb_error_count.argtypes = [c_void_p, POINTER(c_size_t)]

@@ -30,12 +30,12 @@ class Reconstruction:
     errors: np.ndarray
 
     @property
-    def amplitude(self) -> np.ndarray:
-        return np.abs(self.object)
+    def amplitude(self):
+        return abs(self.object)
 
     @property
-    def phase(self) -> np.ndarray:
-        return np.angle(self.object)
+    def phase(self):
+        return self.object.angle() if _is_cuda_tensor(self.object) else np.angle(self.object)
 
     @property
     def error(self) -> float:
@@ -103,6 +103,18 @@ def kernel_launches() -> int:
     return int(_lib.load().qpb_kernel_launches())
 
 
+def _is_cuda_tensor(x) -> bool:
+    """A torch tensor in device memory (the zero-copy path); torch is imported
+    only by callers that pass one."""
+    return type(x).__module__.startswith("torch") and bool(getattr(x, "is_cuda", False))
+
+
+def _torch_stream():
+    import torch
+
+    return torch.cuda.current_stream().cuda_stream
+
+
 def _shape(array: np.ndarray):
     if array.ndim not in (2, 3):
         raise ValueError(f"intensity must be 2D or 3D, got ndim={array.ndim}")
@@ -166,21 +178,63 @@ class Problem:
 
     @property
     def shape(self):
-        return self.amplitude.shape
+        return tuple(self.amplitude.shape)
+
+    @property
+    def on_device(self) -> bool:
+        """True when the arrays are CUDA torch tensors (make_problem of one)."""
+        return _is_cuda_tensor(self.amplitude)
 
     def _c(self):
         p = _lib.Problem()
         p.ndim = self.amplitude.ndim
         p.shape = _lib.shape_arg(self.amplitude.shape)
+        if self.on_device:
+            p.amplitude = ctypes.cast(self.amplitude.data_ptr(), ctypes.POINTER(ctypes.c_float))
+            p.mask = ctypes.cast(self.mask.data_ptr(), ctypes.POINTER(ctypes.c_uint8))
+            p.support = ctypes.cast(self.support.data_ptr(), ctypes.POINTER(ctypes.c_uint8))
+            return p
         p.amplitude = self.amplitude.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         p.mask = self.mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
         p.support = self.support.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
         return p
 
 
+def _make_problem_device(intensity, support, mask, support_threshold):
+    """make_problem on CUDA torch tensors: every array stays on the device."""
+    import torch
+
+    intensity = intensity.detach().to(torch.float32).contiguous()
+    if intensity.dim() not in (2, 3):
+        raise ValueError(f"intensity must be 2D or 3D, got ndim={intensity.dim()}")
+
+    def flag(name, array):
+        if array is None:
+            return None
+        array = torch.as_tensor(array, device=intensity.device)
+        if tuple(array.shape) != tuple(intensity.shape):
+            raise ValueError(f"{name}.shape {tuple(array.shape)} != intensity.shape "
+                             f"{tuple(intensity.shape)}")
+        return (array != 0).to(torch.uint8).contiguous()
+
+    support = flag("support", support)
+    mask = flag("mask", mask)
+    amp = torch.empty_like(intensity)
+    m = torch.empty(intensity.shape, dtype=torch.uint8, device=intensity.device)
+    sup = torch.empty_like(m)
+    ptr = (lambda t: None if t is None else ctypes.c_void_p(t.data_ptr()))
+    _lib.check(_lib.load().qpb_make_problem_device(
+        ptr(intensity), intensity.dim(), _lib.shape_arg(intensity.shape), ptr(support), ptr(mask),
+        support_threshold, ptr(amp), ptr(m), ptr(sup), ctypes.c_void_p(_torch_stream())))
+    return Problem(amp, m, sup)
+
+
 def make_problem(intensity, support=None, mask=None, support_threshold: float = 0.1) -> Problem:
     """Validates the inputs and derives the amplitude; a missing support is the
-    autocorrelation support (src/core/problem.cpp:40-70)."""
+    autocorrelation support (src/core/problem.cpp:40-70). A CUDA torch tensor
+    gives a problem whose arrays stay on the device (no host copy)."""
+    if _is_cuda_tensor(intensity):
+        return _make_problem_device(intensity, support, mask, support_threshold)
     intensity = np.ascontiguousarray(intensity, dtype=np.float32)
     shape = _shape(intensity)
     support = _flag("support", support, intensity.shape)
@@ -215,6 +269,22 @@ def _start(init, shape, starts):
             f"init.shape {init.shape} must be the intensity's {tuple(shape)} or (starts, *shape)"
         )
     return np.ascontiguousarray(init)
+
+
+def _start_device(init, shape, starts):
+    if init is None:
+        return None
+    import torch
+
+    if not _is_cuda_tensor(init):
+        raise ValueError("a device problem takes its init as a CUDA tensor")
+    init = init.to(torch.complex64)
+    if tuple(init.shape) == tuple(shape):
+        init = init.expand(starts, *shape)
+    if tuple(init.shape) != (starts, *shape):
+        raise ValueError(f"init.shape {tuple(init.shape)} must be the intensity's {tuple(shape)} "
+                         "or (starts, *shape)")
+    return init.contiguous()
 
 
 def _ops(recipe):
@@ -265,13 +335,21 @@ class Solver:
                  schedule: Literal["auto", "streamed", "resident"] = "auto"):
         self.problem = problem
         self.shape = problem.shape
-        start = _start(init, problem.shape, starts)
-        options = _options(starts, batch, seed, start, sync_every, variant, amp_storage, device,
-                           stream, schedule)
+        self._on_device = problem.on_device
+        if self._on_device:
+            start = _start_device(init, problem.shape, starts)
+            options = _options(starts, batch, seed, None, sync_every, variant, amp_storage,
+                               device, stream, schedule)
+            if start is not None:
+                options.start = ctypes.cast(start.data_ptr(), ctypes.POINTER(ctypes.c_float))
+        else:
+            start = _start(init, problem.shape, starts)
+            options = _options(starts, batch, seed, start, sync_every, variant, amp_storage,
+                               device, stream, schedule)
         self._lib = _lib.load()
         handle = ctypes.c_void_p()
-        _lib.check(self._lib.qpb_create(ctypes.byref(problem._c()), ctypes.byref(options),
-                                        ctypes.byref(handle)))
+        create = self._lib.qpb_create_device if self._on_device else self._lib.qpb_create
+        _lib.check(create(ctypes.byref(problem._c()), ctypes.byref(options), ctypes.byref(handle)))
         self._handle = handle
         self._progress = None
         if progress is not None:
@@ -316,6 +394,8 @@ class Solver:
         return n.value
 
     def results(self):
+        if self._on_device:
+            return self._results_device()
         starts = self.starts
         count = self.error_count()
         objects = np.empty((starts, *self.shape), np.complex64)
@@ -325,6 +405,21 @@ class Solver:
                                          _lib.ptr(errors)))
         return [Reconstruction(objects[s], supports[s].astype(bool), errors[s])
                 for s in range(starts)]
+
+    def _results_device(self):
+        """Objects and supports as CUDA torch tensors, written by the device."""
+        import torch
+
+        starts = self.starts
+        count = self.error_count()
+        dev = self.problem.amplitude.device
+        objects = torch.empty((starts, *self.shape), dtype=torch.complex64, device=dev)
+        supports = torch.empty((starts, *self.shape), dtype=torch.uint8, device=dev)
+        errors = np.empty((starts, count), np.float32)
+        _lib.check(self._lib.qpb_results_device(
+            self._handle, ctypes.c_void_p(objects.data_ptr()),
+            ctypes.c_void_p(supports.data_ptr()), _lib.ptr(errors)))
+        return [Reconstruction(objects[s], supports[s].bool(), errors[s]) for s in range(starts)]
 
     def close(self):
         if getattr(self, "_handle", None):
@@ -482,7 +577,9 @@ def reconstruct(
     """Array in, reconstruction out.
 
     Args:
-        intensity: measured intensity, centre-origin, 2D or 3D.
+        intensity: measured intensity, centre-origin, 2D or 3D: a numpy array,
+            or a CUDA torch tensor, in which case every array stays on the
+            device and the results' objects and supports are CUDA tensors.
         support: boolean, True inside the object; None derives the
             autocorrelation support.
         mask: boolean, True marks unusable pixels.
@@ -503,10 +600,15 @@ def reconstruct(
             a thread-block cluster's shared memory) or ``"auto"`` (timed once
             per shape and start count).
     """
-    intensity = np.ascontiguousarray(intensity, dtype=np.float32)
-    if intensity.ndim not in (2, 3):
-        raise ValueError(f"intensity must be 2D or 3D, got ndim={intensity.ndim}")
-    negative = float(np.mean(intensity < 0))
+    if _is_cuda_tensor(intensity):
+        if intensity.dim() not in (2, 3):
+            raise ValueError(f"intensity must be 2D or 3D, got ndim={intensity.dim()}")
+        negative = float((intensity < 0).float().mean().item())
+    else:
+        intensity = np.ascontiguousarray(intensity, dtype=np.float32)
+        if intensity.ndim not in (2, 3):
+            raise ValueError(f"intensity must be 2D or 3D, got ndim={intensity.ndim}")
+        negative = float(np.mean(intensity < 0))
     if negative > NEGATIVE_WARN_FRACTION:
         warnings.warn(
             f"{negative:.1%} of intensity pixels are negative and will be clipped to 0; "

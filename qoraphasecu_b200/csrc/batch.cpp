@@ -35,6 +35,9 @@ BatchSolver::BatchSolver(const std::vector<ProblemView>& problems, const SolverO
     where_[q] = {c, static_cast<int>(classes_[c].members.size())};
     classes_[c].members.push_back(static_cast<int>(q));
   }
+  if (options.start && problems[0].on_device && classes_.size() > 1) {
+    throw InvalidArgument("given starts on the device need problems of one shape");
+  }
   std::vector<long long> start_off(problems.size(), 0);
   for (std::size_t q = 1; q < problems.size(); ++q) {
     start_off[q] = start_off[q - 1] + static_cast<long long>(spp_) * numel_[q - 1];
@@ -46,7 +49,7 @@ BatchSolver::BatchSolver(const std::vector<ProblemView>& problems, const SolverO
     o.stream = stream_;
     o.device = select_.device;
     std::vector<float2> given;
-    if (options.start) {
+    if (options.start && classes_.size() > 1) {
       for (int q : c.members) {
         const float2* src = options.start + start_off[q];
         given.insert(given.end(), src, src + static_cast<std::size_t>(spp_) * numel_[q]);
@@ -185,6 +188,11 @@ void BatchSolver::results(float2* objects, std::uint8_t* supports, float* errors
       }
     }
   }
+}
+
+void BatchSolver::results_device(float2* objects, std::uint8_t* supports, float* errors) {
+  if (classes_.size() != 1) throw InvalidArgument("device results need problems of one shape");
+  classes_[0].solver->results_device(objects, supports, errors);
 }
 
 int BatchSolver::profile_passes(int iterations, double* ms) {

@@ -36,6 +36,8 @@ class BatchSolver {
   // Problem order; problem q's block holds starts * numel(q) objects/supports
   // and starts * error_count() errors, blocks back to back.
   void results(float2* objects, std::uint8_t* supports, float* errors);
+  // Objects and supports into device memory (one shape only); errors on the host.
+  void results_device(float2* objects, std::uint8_t* supports, float* errors);
   void set_progress(ProgressFn fn, void* user);
   // One shape class only (the per-pass profile of its solver).
   int profile_passes(int iterations, double* ms);

@@ -11,6 +11,7 @@
 
 #include "../../include/qpb.h"
 #include "batch.hpp"
+#include "device_setup.cuh"
 #include "solver.hpp"
 
 struct qpb_solver {
@@ -228,6 +229,42 @@ qpb_status qpb_create(const qpb_problem* problem, const qpb_options* options, qp
                options->variant, v.shape[0], v.shape[1], v.shape[2]);
     *out = new qpb_solver({v}, o);
     qpb::trace("qpb_create: solver %p ready", static_cast<void*>(*out));
+  });
+}
+
+qpb_status qpb_create_device(const qpb_problem* problem, const qpb_options* options,
+                             qpb_solver** out) {
+  return guarded([&] {
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    const qpb::SolverOptions o = options_of(options);
+    qpb::ProblemView v = made_problem(problem);
+    v.on_device = true;
+    if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
+    *out = new qpb_solver({v}, o);
+  });
+}
+
+qpb_status qpb_results_device(qpb_solver* solver, float* objects, uint8_t* supports,
+                              float* errors) {
+  return guarded([&] {
+    require(solver != nullptr, "solver is NULL");
+    use_solver_device(solver);
+    solver->impl.results_device(reinterpret_cast<float2*>(objects), supports, errors);
+  });
+}
+
+qpb_status qpb_make_problem_device(const float* intensity, int ndim, const int64_t* shape,
+                                   const uint8_t* support, const uint8_t* mask,
+                                   float support_threshold, float* amplitude_out,
+                                   uint8_t* mask_out, uint8_t* support_out, void* stream) {
+  return guarded([&] {
+    numel_checked(ndim, shape);
+    require(intensity && amplitude_out && mask_out && support_out, "NULL array");
+    long long sh[3] = {0, 0, 0};
+    for (int k = 0; k < ndim; ++k) sh[k] = shape[k];
+    qpb::make_problem_device(intensity, ndim, sh, support, mask, support_threshold, amplitude_out,
+                             mask_out, support_out, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -1,0 +1,225 @@
+// Problem set-up from arrays already on the device (callers holding torch or
+// other device tensors): make_problem (src/core/problem.cpp:40-70) with the
+// autocorrelation support (problem.cpp:72-88) computed on the device, and the
+// per-problem preprocessing a solver needs (FFT-order roll, signed amplitude
+// in its storage type and CTA tiling, usable energy), so no array crosses to
+// the host.
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "device_setup.cuh"
+#include "solver.hpp"
+
+namespace qpb {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+int blocks_for(long long work) {
+  return static_cast<int>(std::min<long long>(std::max<long long>((work + kThreads - 1) / kThreads, 1),
+                                              148LL * 8));
+}
+
+#define QPB_LOOP(i, n)                                                              \
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; \
+       i < (n); i += static_cast<long long>(gridDim.x) * blockDim.x)
+
+// amplitude = sqrt(max(I, 0)); mask and support as 0/1; flags[0] counts
+// non-finite intensities, flags[1] masked pixels.
+__global__ void prepare_kernel(const float* intensity, const std::uint8_t* mask,
+                               const std::uint8_t* support, long long n, float* amp,
+                               std::uint8_t* mask_out, std::uint8_t* support_out,
+                               unsigned long long* flags) {
+  unsigned long long bad = 0, masked = 0;
+  QPB_LOOP(i, n) {
+    const float v = intensity[i];
+    if (!isfinite(v)) ++bad;
+    amp[i] = sqrtf(fmaxf(v, 0.0f));
+    const std::uint8_t m = mask ? (mask[i] != 0) : 0;
+    masked += m;
+    mask_out[i] = m;
+    if (support) support_out[i] = support[i] != 0;
+  }
+  if (bad) atomicAdd(flags, bad);
+  if (masked) atomicAdd(flags + 1, masked);
+}
+
+__global__ void to_complex_kernel(const float* in, float2* out, long long n) {
+  QPB_LOOP(i, n) out[i] = {in[i], 0.0f};
+}
+
+// |s w| (FFT order) and its maximum; |.| >= 0, so float bits order like values.
+// Rounded step by step without contraction, exactly as the host computes it.
+__global__ void magnitude_kernel(const float2* w, float* mag, long long n, float s,
+                                 unsigned* max_bits) {
+  float best = 0.0f;
+  QPB_LOOP(i, n) {
+    const float2 v = w[i];
+    const float re = __fmul_rn(v.x, s), im = __fmul_rn(v.y, s);
+    const float m = sqrtf(__fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im)));
+    mag[i] = m;
+    best = fmaxf(best, m);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(max_bits, __float_as_uint(best));
+}
+
+__global__ void threshold_kernel(const float* mag, long long n, const unsigned* max_bits,
+                                 float threshold, std::uint8_t* out) {
+  const float level = __fmul_rn(threshold, __uint_as_float(*max_bits));
+  QPB_LOOP(i, n) out[i] = mag[i] > level;
+}
+
+// Element e (FFT order) of one problem goes to index `tiled(e)` of the
+// signed-amplitude array: the modulus pass's CTA order for columns (element j
+// of line c of CTA tile t at (t * L + j) * lines + c), FFT order otherwise.
+__device__ __forceinline__ long long tiled_index(long long e, int L, int S, int lines) {
+  if (lines <= 0 || S == 1) return e;
+  const long long slab = static_cast<long long>(L) * S;
+  const long long outer = e / slab;
+  const long long rem = e - outer * slab;
+  const long long j = rem / S;
+  const long long col = rem - j * S;
+  const long long tile = outer * (S / lines) + col / lines;
+  return (tile * L + j) * lines + col % lines;
+}
+
+template <class T>
+__device__ __forceinline__ T from_float(float v);
+template <>
+__device__ __forceinline__ float from_float<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __half from_float<__half>(float v) { return __float2half_rn(v); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_float<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+
+template <class T>
+__global__ void signed_kernel(const float* amp, const std::uint8_t* mask, long long n, int L, int S,
+                              int lines, T* out) {
+  QPB_LOOP(e, n) out[tiled_index(e, L, S, lines)] = from_float<T>(mask[e] ? -1.0f : amp[e]);
+}
+
+__global__ void nonzero_kernel(std::uint8_t* v, long long n) {
+  QPB_LOOP(i, n) v[i] = v[i] != 0;
+}
+
+__global__ void energy_kernel(const float* amp, const std::uint8_t* mask, long long n, double* out) {
+  __shared__ double partial[kThreads / 32];
+  double e = 0.0;
+  QPB_LOOP(i, n) {
+    if (!mask[i]) e += static_cast<double>(amp[i]) * amp[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += partial[w];
+    atomicAdd(out, t);
+  }
+}
+
+}  // namespace
+
+void make_problem_device(const float* intensity, int ndim, const long long* shape,
+                         const std::uint8_t* support, const std::uint8_t* mask,
+                         float support_threshold, float* amplitude_out, std::uint8_t* mask_out,
+                         std::uint8_t* support_out, cudaStream_t stream) {
+  ProblemView v;
+  v.ndim = ndim;
+  for (int a = 0; a < ndim && a < 3; ++a) v.shape[a] = shape[a];
+  const Dims3 d = dims_of(v);
+  const long long n = d.n();
+  DeviceBuffer<unsigned long long> flags(2);
+  QPB_CHECK(cudaMemsetAsync(flags.get(), 0, 2 * sizeof(unsigned long long), stream));
+  prepare_kernel<<<blocks_for(n), kThreads, 0, stream>>>(intensity, mask, support, n, amplitude_out,
+                                                          mask_out, support_out, flags.get());
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+  // Without a support: |IFFT(I)| in FFT order, centre-origin again, > threshold * max.
+  PlanCache plans;
+  DeviceBuffer<float> ordered(support ? 0 : static_cast<std::size_t>(n));
+  DeviceBuffer<float> mag(support ? 0 : static_cast<std::size_t>(n));
+  DeviceBuffer<float2> w(support ? 0 : static_cast<std::size_t>(n));
+  DeviceBuffer<unsigned> max_bits(1);
+  if (!support) {
+    PassRunner runner(d, ndim, plans);
+    QPB_CHECK(cudaMemsetAsync(max_bits.get(), 0, sizeof(unsigned), stream));
+    roll<float>(intensity, ordered.get(), d, 1, true, stream);
+    to_complex_kernel<<<blocks_for(n), kThreads, 0, stream>>>(ordered.get(), w.get(), n);
+    QPB_CHECK(cudaGetLastError());
+    for (int axis3 = runner.outer(); axis3 < 3; ++axis3) {
+      PassParams p = runner.params(Mode::kInv, axis3, 1);
+      p.w = w.get();
+      p.x = w.get();
+      runner.launch(Mode::kInv, axis3, p, stream);
+    }
+    magnitude_kernel<<<blocks_for(n), kThreads, 0, stream>>>(
+        w.get(), ordered.get(), n, 1.0f / std::sqrt(static_cast<float>(n)), max_bits.get());
+    QPB_CHECK(cudaGetLastError());
+    roll<float>(ordered.get(), mag.get(), d, 1, false, stream);
+    threshold_kernel<<<blocks_for(n), kThreads, 0, stream>>>(mag.get(), n, max_bits.get(),
+                                                             support_threshold, support_out);
+    QPB_CHECK(cudaGetLastError());
+    count_launches(3);
+  }
+  unsigned long long host_flags[2];
+  QPB_CHECK(cudaMemcpyAsync(host_flags, flags.get(), sizeof(host_flags), cudaMemcpyDeviceToHost,
+                            stream));
+  QPB_CHECK(cudaStreamSynchronize(stream));
+  check_waits();
+  if (host_flags[0]) throw InvalidArgument("intensity contains NaN or Inf");
+  if (mask && host_flags[1] == static_cast<unsigned long long>(n)) {
+    throw InvalidArgument("mask marks every pixel as bad; nothing left to fit");
+  }
+}
+
+double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
+                              int lines, float* amp_fft, void* signed_out,
+                              std::uint8_t* support_fft, cudaStream_t stream) {
+  const long long n = d.n();
+  DeviceBuffer<std::uint8_t> mask_fft(static_cast<std::size_t>(n));
+  DeviceBuffer<double> energy(1);
+  roll<float>(q.amplitude, amp_fft, d, 1, true, stream);
+  if (q.mask) {
+    roll<std::uint8_t>(q.mask, mask_fft.get(), d, 1, true, stream);
+  } else {
+    QPB_CHECK(cudaMemsetAsync(mask_fft.get(), 0, static_cast<std::size_t>(n), stream));
+  }
+  roll<std::uint8_t>(q.support, support_fft, d, 1, true, stream);
+  nonzero_kernel<<<blocks_for(n), kThreads, 0, stream>>>(support_fft, n);
+  QPB_CHECK(cudaGetLastError());
+  QPB_CHECK(cudaMemsetAsync(energy.get(), 0, sizeof(double), stream));
+  switch (storage) {
+    case AmpStorage::kF32:
+      signed_kernel<float><<<blocks_for(n), kThreads, 0, stream>>>(
+          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<float*>(signed_out));
+      break;
+    case AmpStorage::kF16:
+      signed_kernel<__half><<<blocks_for(n), kThreads, 0, stream>>>(
+          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<__half*>(signed_out));
+      break;
+    case AmpStorage::kBF16:
+      signed_kernel<__nv_bfloat16><<<blocks_for(n), kThreads, 0, stream>>>(
+          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<__nv_bfloat16*>(signed_out));
+      break;
+  }
+  QPB_CHECK(cudaGetLastError());
+  energy_kernel<<<blocks_for(n), kThreads, 0, stream>>>(amp_fft, mask_fft.get(), n, energy.get());
+  QPB_CHECK(cudaGetLastError());
+  count_launches(3);
+  double host = 0.0;
+  QPB_CHECK(cudaMemcpyAsync(&host, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
+  QPB_CHECK(cudaStreamSynchronize(stream));
+  return host;
+}
+
+}  // namespace qpb

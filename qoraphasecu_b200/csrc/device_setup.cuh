@@ -1,0 +1,34 @@
+// Problem set-up from arrays already on the device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "line_pass.cuh"
+
+namespace qpb {
+
+struct ProblemView;
+struct Dims3;
+
+// make_problem (src/core/problem.cpp:40-70) on device arrays, centre-origin:
+// amplitude = sqrt(max(I, 0)), mask and support as 0/1, a NULL support
+// replaced by the autocorrelation support at `support_threshold` (computed on
+// the device). Enqueued on `stream`; returns after it, raising
+// InvalidArgument for non-finite intensities or a mask that covers everything.
+void make_problem_device(const float* intensity, int ndim, const long long* shape,
+                         const std::uint8_t* support, const std::uint8_t* mask,
+                         float support_threshold, float* amplitude_out, std::uint8_t* mask_out,
+                         std::uint8_t* support_out, cudaStream_t stream);
+
+// One problem's solver inputs from its device arrays (centre-origin): the FFT-
+// order FP32 amplitude, the signed amplitude (-1 masked) in `storage` written
+// to `signed_out` in the modulus pass's CTA order when `lines` > 0 and S > 1,
+// and the FFT-order 0/1 support. Returns the usable energy (sum of A^2 over
+// unmasked pixels); synchronises `stream`.
+double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
+                              int lines, float* amp_fft, void* signed_out,
+                              std::uint8_t* support_fft, cudaStream_t stream);
+
+}  // namespace qpb

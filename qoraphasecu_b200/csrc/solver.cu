@@ -15,6 +15,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "device_setup.cuh"
 #include "fast_pass.cuh"
 #include "resident.cuh"
 #include "solver.hpp"
@@ -314,7 +315,11 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   std::vector<float> amp_all;
   std::vector<unsigned char> signed_all;
   std::vector<std::vector<std::uint8_t>> supports;
+  const bool on_device = problem.on_device;
   for (const ProblemView& q : problems) {
+    if (q.on_device != on_device) throw InvalidArgument("problems mix host and device arrays");
+  }
+  for (const ProblemView& q : (on_device ? std::vector<ProblemView>{} : problems)) {
     const auto amp = host_roll(q.amplitude, d_, true);
     std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
     if (q.mask) {
@@ -334,12 +339,28 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
     supports.push_back(std::move(sup));
   }
   amp_tiled_ = tile;
-  amp_ = upload(signed_all, stream_);
-
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  support_ = DeviceBuffer<std::uint8_t>(total);
+  DeviceBuffer<float> amp_f;  // FP32 FFT-order amplitude of every problem, for the random starts
+  if (on_device) {
+    // The same preparation on the device, from the caller's device arrays.
+    const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
+    amp_f = DeviceBuffer<float>(static_cast<std::size_t>(problems_) * n_);
+    amp_ = DeviceBuffer<unsigned char>(static_cast<std::size_t>(problems_) * n_ * elem);
+    for (int q = 0; q < problems_; ++q) {
+      energies_.push_back(prepare_problem_device(
+          problems[q], d_, options.amp_storage, mod.L, mod.S, tile ? lines : 0,
+          amp_f.get() + static_cast<std::size_t>(q) * n_,
+          amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
+          support_.get() + static_cast<std::size_t>(q) * spp_ * n_, stream_));
+    }
+  } else {
+    amp_ = upload(signed_all, stream_);
+    amp_f = upload(amp_all, stream_);
+  }
+
   x_ = DeviceBuffer<float2>(total);
   w_ = DeviceBuffer<float2>(total);
-  support_ = DeviceBuffer<std::uint8_t>(total);
   saved_ = DeviceBuffer<std::uint8_t>(total);
   level_ = DeviceBuffer<LevelAcc>(static_cast<std::size_t>(batch_));
   moments_ = DeviceBuffer<unsigned long long>(2 * static_cast<std::size_t>(starts_));
@@ -351,8 +372,10 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   set_ctrl(ctrl_.get(), ctrl, stream_);
   for (int q = 0; q < problems_; ++q) {
     std::uint8_t* first = support_.get() + static_cast<std::size_t>(q) * spp_ * n_;
-    QPB_CHECK(cudaMemcpyAsync(first, supports[q].data(), supports[q].size(),
-                              cudaMemcpyHostToDevice, stream_));
+    if (!on_device) {
+      QPB_CHECK(cudaMemcpyAsync(first, supports[q].data(), supports[q].size(),
+                                cudaMemcpyHostToDevice, stream_));
+    }
     for (int s = 1; s < spp_; ++s) {
       QPB_CHECK(cudaMemcpyAsync(first + static_cast<std::size_t>(s) * n_, first,
                                 static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
@@ -363,8 +386,8 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
 
   if (options.start) {
     // Given starts, centre-origin: to FFT order, cut to the support (cpu_solver.cpp:37-41).
-    QPB_CHECK(cudaMemcpyAsync(w_.get(), options.start, total * sizeof(float2),
-                              cudaMemcpyHostToDevice, stream_));
+    QPB_CHECK(cudaMemcpyAsync(w_.get(), options.start, total * sizeof(float2), cudaMemcpyDefault,
+                              stream_));
     roll<float2>(w_.get(), x_.get(), d_, starts_, true, stream_);
     support_project(x_.get(), support_.get(), n_, starts_, stream_);
     wave_valid_ = false;
@@ -372,7 +395,6 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   } else {
     // Random phases on the measured amplitude, inverse transform, cut to the
     // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
-    auto amp_f = upload(amp_all, stream_);
     for (int g = 0; g < groups_; ++g) {
       random_wave(w(g), amp_f.get(), amp_stride_, spp_, n_, batch_, options.seed,
                   static_cast<std::uint64_t>(g) * batch_, stream_);
@@ -733,6 +755,18 @@ std::vector<float> Solver::latest_errors() {
 void Solver::report() {
   const std::vector<float> latest = latest_errors();
   progress_(progress_user_, iteration_, latest.data(), starts_);
+}
+
+void Solver::results_device(float2* objects, std::uint8_t* supports, float* errors) {
+  if (objects) roll<float2>(x_.get(), objects, d_, starts_, false, stream_);
+  if (supports) roll<std::uint8_t>(support_.get(), supports, d_, starts_, false, stream_);
+  stream_.sync();
+  if (errors) {
+    const std::size_t count = error_count();
+    for (int s = 0; s < starts_; ++s) {
+      std::copy(errors_[s].begin(), errors_[s].end(), errors + static_cast<std::size_t>(s) * count);
+    }
+  }
 }
 
 void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {

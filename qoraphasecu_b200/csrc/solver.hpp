@@ -99,6 +99,7 @@ struct ProblemView {
   const float* amplitude = nullptr;     // sqrt(clip(I, 0)), numel
   const std::uint8_t* mask = nullptr;   // 1 = unusable; null = none
   const std::uint8_t* support = nullptr;  // 1 = inside
+  bool on_device = false;               // the arrays are device pointers
 };
 
 enum class Variant : int {
@@ -215,6 +216,9 @@ class Solver {
   cudaStream_t stream() const { return stream_; }
   // objects: starts * numel complex64; supports: starts * numel; errors: starts * error_count().
   void results(float2* objects, std::uint8_t* supports, float* errors);
+  // As results(), objects and supports written to device memory (centre-origin)
+  // on the solver's stream, which is synchronised before returning; errors on the host.
+  void results_device(float2* objects, std::uint8_t* supports, float* errors);
   void set_progress(ProgressFn fn, void* user) {
     progress_ = fn;
     progress_user_ = user;
