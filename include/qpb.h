@@ -263,6 +263,15 @@ QPB_API qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int b
 QPB_API qpb_status qpb_aligned_error(const float* a, const float* reference, int ndim,
                                      const int64_t* shape, int batch, float* out);
 
+/* Ensemble alignment and averaging (no counterpart in the reference, whose
+ * README.md:222-224 leaves it to the user): the alignment of qpb_aligned_error
+ * applied. errors: batch floats as qpb_aligned_error (may be NULL); aligned:
+ * batch * numel complex64, object b -- or its twin, whichever fits better --
+ * translated and phase-rotated onto the reference (may be NULL); mean: numel
+ * complex64, the average of the aligned objects (may be NULL). Host arrays. */
+QPB_API qpb_status qpb_align(const float* a, const float* reference, int ndim, const int64_t* shape,
+                             int batch, float* errors, float* aligned, float* mean);
+
 /* qpcu::simulate_intensity (problem.hpp:42, problem.cpp:90-99): |centred unitary
  * FFT(object)|^2 of a centre-origin complex64 object, the transform on the
  * device. Host arrays of numel elements. */

@@ -17,6 +17,7 @@ from .api import (
     Problem,
     Reconstruction,
     Solver,
+    align,
     aligned_error,
     autocorrelation_support,
     best_index,
@@ -43,6 +44,7 @@ __all__ = [
     "Reconstruction",
     "Shrinkwrap",
     "Solver",
+    "align",
     "aligned_error",
     "autocorrelation_support",
     "best_index",

@@ -60,6 +60,7 @@ EXPORTS = (
     "qpb_amplitude_loss_grad",
     "qpb_modulus_project_noalloc",
     "qpb_aligned_error",
+    "qpb_align",
     "qpb_simulate_intensity",
     "qpb_modulus_project",
     "qpb_support_project",
@@ -164,6 +165,8 @@ def load():
         lib.qpb_support_project.argtypes = [c_void_p, c_void_p, c_size_t]
         lib.qpb_aligned_error.argtypes = [c_void_p, c_void_p, c_int, POINTER(c_int64), c_int,
                                           c_void_p]
+        lib.qpb_align.argtypes = [c_void_p, c_void_p, c_int, POINTER(c_int64), c_int, c_void_p,
+                                  c_void_p, c_void_p]
         lib.qpb_simulate_intensity.argtypes = [c_void_p, c_int, POINTER(c_int64), c_void_p]
         lib.qpb_gaussian_blur.argtypes = [c_void_p, c_int, POINTER(c_int64), c_float, c_void_p]
         _lib = lib

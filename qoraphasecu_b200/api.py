@@ -67,6 +67,16 @@ class Ensemble:
     def best(self) -> Reconstruction:
         return self.runs[best_index(self.runs)]
 
+    def average(self, runs: int | None = None):
+        """The mean of the ``runs`` best runs (all by default), each translated,
+        twin-flipped if that fits better and phase-rotated onto the best run
+        (device alignment, :func:`align`). Returns ``(mean, aligned errors)``."""
+        order = self.ranking[: runs or len(self.runs)]
+        host = (lambda o: o.detach().cpu().numpy() if _is_cuda_tensor(o) else np.asarray(o))
+        stack = np.stack([host(self.runs[i].object) for i in order])
+        _, mean, errors = align(stack, stack[0])
+        return mean, errors
+
 
 def best_index(runs) -> int:
     """Index of the run with the lowest final error; a NaN run never displaces a
@@ -156,6 +166,24 @@ def aligned_error(a, reference):
     _lib.check(_lib.load().qpb_aligned_error(_lib.ptr(a), _lib.ptr(reference), reference.ndim,
                                              _shape(reference), batch, _lib.ptr(out)))
     return out if stacked else float(out[0])
+
+
+def align(objects, reference):
+    """Moves every object of a stack ``(batch, *shape)`` onto ``reference``: the
+    translation (cross-correlation peak), twin and global phase that
+    ``aligned_error`` finds, applied on the device. Returns ``(aligned,
+    mean, errors)``: the aligned stack, its average and the aligned errors."""
+    objects = np.ascontiguousarray(objects, dtype=np.complex64)
+    reference = np.ascontiguousarray(reference, dtype=np.complex64)
+    if objects.ndim != reference.ndim + 1 or objects.shape[1:] != reference.shape:
+        raise ValueError(f"objects.shape {objects.shape} is not a stack of {reference.shape}")
+    aligned = np.empty_like(objects)
+    mean = np.empty_like(reference)
+    errors = np.empty(objects.shape[0], np.float32)
+    _lib.check(_lib.load().qpb_align(_lib.ptr(objects), _lib.ptr(reference), reference.ndim,
+                                     _shape(reference), objects.shape[0], _lib.ptr(errors),
+                                     _lib.ptr(aligned), _lib.ptr(mean)))
+    return aligned, mean, errors
 
 
 def simulate_intensity(obj) -> np.ndarray:
@@ -637,6 +665,7 @@ __all__ = [
     "Recipe",
     "Reconstruction",
     "Solver",
+    "align",
     "aligned_error",
     "autocorrelation_support",
     "best_index",

@@ -370,6 +370,20 @@ qpb_status qpb_aligned_error(const float* a, const float* reference, int ndim,
   });
 }
 
+qpb_status qpb_align(const float* a, const float* reference, int ndim, const int64_t* shape,
+                     int batch, float* errors, float* aligned, float* mean) {
+  return guarded([&] {
+    require(a && reference, "NULL array");
+    numel_checked(ndim, shape);
+    require(batch >= 1, "batch must be >= 1");
+    long long sh[3] = {0, 0, 0};
+    for (int k = 0; k < ndim; ++k) sh[k] = shape[k];
+    qpb::align(reinterpret_cast<const float2*>(a), reinterpret_cast<const float2*>(reference), ndim,
+               sh, batch, errors, reinterpret_cast<float2*>(aligned),
+               reinterpret_cast<float2*>(mean));
+  });
+}
+
 qpb_status qpb_simulate_intensity(const float* object, int ndim, const int64_t* shape,
                                   float* out) {
   return guarded([&] {

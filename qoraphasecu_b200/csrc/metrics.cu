@@ -151,6 +151,43 @@ __global__ void overlap_kernel(const float2* ref, const float2* cand, Dims3 d,
   }
 }
 
+// out[b][i] = rotation_c * cand[c][shifted_source(i)] for the chosen
+// candidate c of object b (its direct form or its twin), rotation_c =
+// overlap_c / |overlap_c|: object b moved onto the reference.
+__global__ void apply_kernel(const float2* cand, Dims3 d, const unsigned long long* key,
+                             const double* acc, const int* choice, float2* out) {
+  const long long n = d.n();
+  const int b = blockIdx.y;
+  const int c = choice[b];
+  const float2* src = cand + c * n;
+  const double* a = acc + 4 * c;
+  const long long peak = static_cast<long long>(0xffffffffULL - (key[c] & 0xffffffffULL));
+  const double mag = sqrt(a[0] * a[0] + a[1] * a[1]);
+  const float rr = mag > 0.0 ? static_cast<float>(a[0] / mag) : 1.0f;
+  const float ri = mag > 0.0 ? static_cast<float>(a[1] / mag) : 0.0f;
+  out += b * n;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const float2 s = src[shifted_source(i, d, peak)];
+    out[i] = {rr * s.x - ri * s.y, rr * s.y + ri * s.x};
+  }
+}
+
+// mean[i] = (1 / batch) sum_b aligned[b][i], summed in order of b.
+__global__ void mean_kernel(const float2* aligned, long long n, int batch, float2* mean) {
+  const float inv = 1.0f / static_cast<float>(batch);
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    float2 sum = {0.0f, 0.0f};
+    for (int b = 0; b < batch; ++b) {
+      const float2 v = aligned[b * n + i];
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    mean[i] = {sum.x * inv, sum.y * inv};
+  }
+}
+
 __global__ void intensity_kernel(const float2* w, float* out, long long n, float scale2) {
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -189,8 +226,8 @@ ProblemView shape_view(int ndim, const long long* shape) {
 
 }  // namespace
 
-void aligned_error(const float2* a, const float2* reference, int ndim, const long long* shape,
-                   int batch, float* out) {
+void align(const float2* a, const float2* reference, int ndim, const long long* shape, int batch,
+           float* errors, float2* aligned, float2* mean) {
   if (batch < 1) throw InvalidArgument("batch must be >= 1");
   const Dims3 d = dims_of(shape_view(ndim, shape));
   const long long n = d.n();
@@ -232,15 +269,40 @@ void aligned_error(const float2* a, const float2* reference, int ndim, const lon
                             cudaMemcpyDeviceToHost, s));
   s.sync();
   check_waits();
+  std::vector<int> choice(static_cast<std::size_t>(batch));
   for (int b = 0; b < batch; ++b) {
-    float best = 0.0f;
+    float e[2];
     for (int k = 0; k < 2; ++k) {
       const double* v = host.data() + 4 * (b + k * batch);
-      const float e = static_cast<float>(std::sqrt(v[3] / std::max(v[2], DBL_MIN)));
-      best = k == 0 ? e : std::min(best, e);
+      e[k] = static_cast<float>(std::sqrt(v[3] / std::max(v[2], DBL_MIN)));
     }
-    out[b] = best;
+    choice[b] = e[0] <= e[1] ? b : b + batch;
+    if (errors) errors[b] = std::min(e[0], e[1]);
   }
+  if (!aligned && !mean) return;
+  // The chosen candidate of every object, moved onto the reference, and their mean.
+  DeviceBuffer<int> chosen(static_cast<std::size_t>(batch));
+  QPB_CHECK(cudaMemcpyAsync(chosen.get(), choice.data(), choice.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  apply_kernel<<<grid_b, kThreads, 0, s>>>(cand.get(), d, key.get(), acc.get(), chosen.get(),
+                                          corr.get());
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+  if (mean) {
+    mean_kernel<<<blocks_for(n), kThreads, 0, s>>>(corr.get(), n, batch, fr.get());
+    QPB_CHECK(cudaGetLastError());
+    count_launches(1);
+    QPB_CHECK(cudaMemcpyAsync(mean, fr.get(), bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if (aligned) {
+    QPB_CHECK(cudaMemcpyAsync(aligned, corr.get(), bytes * batch, cudaMemcpyDeviceToHost, s));
+  }
+  s.sync();
+}
+
+void aligned_error(const float2* a, const float2* reference, int ndim, const long long* shape,
+                   int batch, float* out) {
+  align(a, reference, ndim, shape, batch, out, nullptr, nullptr);
 }
 
 void simulate_intensity(const float2* object, int ndim, const long long* shape, float* out) {

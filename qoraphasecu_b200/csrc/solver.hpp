@@ -319,6 +319,12 @@ void autocorrelation_support(const float* intensity, int ndim, const long long* 
 // direct and twin errors. Host arrays.
 void aligned_error(const float2* a, const float2* reference, int ndim, const long long* shape,
                    int batch, float* out);
+// The same alignment, also applied: errors[b] as aligned_error (may be null),
+// aligned[b] = object b (or its twin, whichever fits better) translated and
+// phase-rotated onto the reference (batch * numel, may be null), mean = their
+// average (numel, may be null). Host arrays.
+void align(const float2* a, const float2* reference, int ndim, const long long* shape, int batch,
+           float* errors, float2* aligned, float2* mean);
 // simulate_intensity (problem.cpp:90-99): |centred unitary FFT(object)|^2 of a
 // centre-origin complex64 object, FFT on the device. Host arrays.
 void simulate_intensity(const float2* object, int ndim, const long long* shape, float* out);

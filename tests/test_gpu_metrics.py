@@ -61,3 +61,55 @@ def test_aligned_error_scores_reconstructions(gpu):
 def test_shape_mismatch_is_a_value_error(gpu):
     with pytest.raises(ValueError, match="shapes differ"):
         qpc.aligned_error(np.zeros((8, 8), np.complex64), np.zeros((8, 9), np.complex64))
+
+
+def numpy_align(a, ref):
+    """The translation, twin and phase of src/core/metrics.cpp:17-86, applied
+    with numpy complex128 (the same steps as the oracle's aligned_error)."""
+    axes = tuple(range(ref.ndim))
+    best = None
+    for cand in (a, np.roll(np.conj(np.flip(a, axis=axes)), 1, axis=axes)):
+        cand = cand.astype(np.complex128)
+        cc = np.fft.ifftn(np.fft.fftn(ref) * np.conj(np.fft.fftn(cand)))
+        shift = np.unravel_index(int(np.argmax(np.abs(cc) ** 2)), ref.shape)
+        moved = np.roll(cand, shift, axis=axes)
+        overlap = np.sum(ref * np.conj(moved))
+        moved = moved * (overlap / abs(overlap))
+        err = np.linalg.norm(moved - ref) / np.linalg.norm(ref)
+        if best is None or err < best[1]:
+            best = (moved, err)
+    return best
+
+
+@pytest.mark.parametrize("shape", [(64, 48), (21, 15), (16, 20, 12)])
+def test_align_moves_every_object_onto_the_reference(gpu, shape):
+    n = int(np.prod(shape))
+    axes = tuple(range(len(shape)))
+    ref = random_field(n, 1).reshape(shape)
+    rng = np.random.default_rng(3)
+    objs = []
+    for k in range(4):
+        shift = tuple(int(rng.integers(0, s)) for s in shape)
+        o = np.roll(ref, shift, axis=axes) * np.exp(1j * rng.uniform(-3, 3))
+        if k % 2:
+            o = np.conj(np.flip(o, axis=axes))
+        objs.append((o + 1e-3 * random_field(n, 10 + k).reshape(shape)).astype(np.complex64))
+    stack = np.stack(objs)
+    aligned, mean, errors = qpc.align(stack, ref)
+    np.testing.assert_allclose(errors, qpc.aligned_error(stack, ref), rtol=1e-6)
+    for a, o in zip(aligned, objs, strict=True):
+        expected, err = numpy_align(o, ref.astype(np.complex128))
+        assert fp64.relative_diff(a, expected) < 1e-5
+        assert fp64.relative_diff(a, ref) < 2e-3
+    assert fp64.relative_diff(mean, np.mean(aligned.astype(np.complex128), axis=0)) < 1e-6
+    assert fp64.relative_diff(mean, ref) < 1e-3
+
+
+def test_ensemble_average(gpu):
+    obj, support, intensity = triangle((64, 64), 20)
+    ens = qpc.reconstruct(intensity, support=support, starts=4, seed=2)
+    mean, errors = ens.average()
+    assert mean.shape == obj.shape and errors.shape == (4,)
+    assert errors[0] < 1e-6  # the best run against itself
+    one, e1 = ens.average(runs=1)
+    np.testing.assert_allclose(one, ens.best.object, rtol=0, atol=1e-6)
