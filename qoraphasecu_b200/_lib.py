@@ -48,6 +48,7 @@ EXPORTS = (
     "qpb_make_problem_device",
     "qpb_create_device",
     "qpb_results_device",
+    "qpb_reset",
     "qpb_run",
     "qpb_set_progress",
     "qpb_error_count",
@@ -147,6 +148,7 @@ def load():
         lib.qpb_create_device.argtypes = [POINTER(Problem), POINTER(Options), POINTER(c_void_p)]
         lib.qpb_results_device.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_run.argtypes = [c_void_p, POINTER(Op), c_size_t]
+        lib.qpb_reset.argtypes = [c_void_p, POINTER(Problem), c_size_t, c_uint64, c_void_p]
         lib.qpb_set_progress.argtypes = [c_void_p, PROGRESS, c_void_p]
         lib.qpb_error_count.argtypes = [c_void_p, POINTER(c_size_t)]
         lib.qpb_starts.argtypes = [c_void_p, POINTER(c_int)]

@@ -9,6 +9,7 @@ Mirrors the reference's ``python/qoraphasecu/api.py`` (``reconstruct`` at
 from __future__ import annotations
 
 import ctypes
+import threading
 import warnings
 from dataclasses import dataclass
 from typing import Literal
@@ -97,8 +98,10 @@ def cuda_available() -> bool:
 
 
 def set_device(device: int) -> None:
-    """Device used on this thread by calls without a solver (make_problem, operators)."""
+    """Device used on this thread by calls without a solver (make_problem,
+    operators) and by reconstruct()."""
     _lib.check(_lib.load().qpb_set_device(device))
+    _cache.device = device
 
 
 def tuning_report() -> str:
@@ -400,6 +403,27 @@ class Solver:
         ops, count = _ops(default_recipe() if recipe is None else recipe)
         _lib.check(self._lib.qpb_run(self._handle, ops, count))
 
+    def reset(self, problem: Problem, *, seed: int | None = None, init=None):
+        """Loads a new problem of the same shape (host or device arrays, as at
+        construction) and draws new starts (or takes ``init``), keeping the
+        device buffers, schedule and captured graphs: the cheap way to run many
+        same-shape reconstructions. Error histories start afresh."""
+        if tuple(problem.shape) != tuple(self.shape):
+            raise ValueError(f"problem.shape {tuple(problem.shape)} != solver shape "
+                             f"{tuple(self.shape)}")
+        if problem.on_device != self._on_device:
+            raise ValueError("reset takes the same kind of arrays (host or device) as construction")
+        starts = self.starts
+        if self._on_device:
+            start = _start_device(init, problem.shape, starts)
+            ptr = None if start is None else ctypes.c_void_p(start.data_ptr())
+        else:
+            start = _start(init, problem.shape, starts)
+            ptr = None if start is None else ctypes.c_void_p(start.ctypes.data)
+        _lib.check(self._lib.qpb_reset(self._handle, ctypes.byref(problem._c()), 1,
+                                       0 if seed is None else seed, ptr))
+        self.problem = problem
+
     def profile_passes(self, iterations: int = 20):
         """Mean device time (ms) of each line pass of one iteration, timed with
         CUDA events around direct launches; with the resident schedule, one
@@ -650,12 +674,47 @@ def reconstruct(
     if recipe is None:
         recipe = default_recipe()
     problem = make_problem(intensity, support, mask, support_threshold)
-    with Solver(problem, starts=starts, batch=batch, seed=seed, init=init, sync_every=sync_every,
-                variant=variant, amp_storage=amp_storage, progress=progress,
-                schedule=schedule) as solver:
-        solver.run(recipe)
-        runs = solver.results()
+    key = (tuple(problem.shape), problem.on_device, starts, batch, sync_every, variant,
+           amp_storage, schedule, _current_device())
+    solver = _cached_solvers().get(key)
+    if solver is not None and solver._handle:
+        solver.reset(problem, seed=seed, init=init)
+    else:
+        solver = Solver(problem, starts=starts, batch=batch, seed=seed, init=init,
+                        sync_every=sync_every, variant=variant, amp_storage=amp_storage,
+                        schedule=schedule)
+        _cached_solvers()[key] = solver
+    solver.set_progress(progress)
+    solver.run(recipe)
+    runs = solver.results()
+    solver.set_progress(None)
     return runs[0] if starts == 1 else Ensemble(tuple(runs))
+
+
+_cache = threading.local()
+
+
+def _cached_solvers() -> dict:
+    """reconstruct() keeps the solver of its last call per configuration and
+    thread, and loads the next same-shape problem into it (Solver.reset):
+    allocation and graph capture are paid once. clear_cache() releases them."""
+    if not hasattr(_cache, "solvers"):
+        _cache.solvers = {}
+    return _cache.solvers
+
+
+def clear_cache() -> None:
+    """Releases the solvers (and their device memory) that reconstruct() keeps
+    for reuse on this thread."""
+    for solver in _cached_solvers().values():
+        solver.close()
+    _cached_solvers().clear()
+
+
+def _current_device() -> int:
+    """The device set by set_device() on this thread (-1: never set), part of
+    the reconstruct cache key."""
+    return getattr(_cache, "device", -1)
 
 
 __all__ = [
@@ -675,4 +734,5 @@ __all__ = [
     "reconstruct",
     "reconstruct_batch",
     "simulate_intensity",
+    "clear_cache",
 ]

@@ -14,7 +14,8 @@ BatchSolver::BatchSolver(const std::vector<ProblemView>& problems, const SolverO
       stream_(options.stream),
       spp_(options.starts),
       every_(options.sync_every),
-      batched_(options.variant == Variant::kBatched) {
+      batched_(options.variant == Variant::kBatched),
+      on_device_(!problems.empty() && problems[0].on_device) {
   if (problems.empty()) throw InvalidArgument("no problems");
   if (options.starts < 1) throw InvalidArgument("starts must be >= 1");
   if (options.sync_every < 1) throw InvalidArgument("sync_every must be >= 1");
@@ -188,6 +189,14 @@ void BatchSolver::results(float2* objects, std::uint8_t* supports, float* errors
       }
     }
   }
+}
+
+void BatchSolver::reset(std::vector<ProblemView> problems, std::uint64_t seed,
+                        const float2* start) {
+  if (classes_.size() != 1) throw InvalidArgument("reset needs problems of one shape");
+  for (ProblemView& q : problems) q.on_device = on_device_;
+  classes_[0].solver->reset(problems, seed, start);
+  iteration_ = 0;
 }
 
 void BatchSolver::results_device(float2* objects, std::uint8_t* supports, float* errors) {

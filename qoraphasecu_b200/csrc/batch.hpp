@@ -28,6 +28,10 @@ class BatchSolver {
   BatchSolver& operator=(const BatchSolver&) = delete;
 
   void run(const OpDesc* ops, std::size_t count);
+  // Solver::reset for a batch of one shape class: new problems (same count and
+  // shape, host or device arrays as at construction), new starts.
+  void reset(std::vector<ProblemView> problems, std::uint64_t seed, const float2* start);
+  bool on_device() const { return on_device_; }
   std::size_t error_count() const { return classes_[0].solver->error_count(); }
   int starts() const { return spp_ * static_cast<int>(where_.size()); }
   int problems() const { return static_cast<int>(where_.size()); }
@@ -54,6 +58,7 @@ class BatchSolver {
   int spp_;
   int every_;
   bool batched_;  // chunks captured into graphs (else launched directly)
+  bool on_device_;  // problem arrays given as device pointers
   std::vector<Class> classes_;
   std::vector<std::pair<int, int>> where_;  // problem -> (class, index in class)
   std::vector<long long> numel_;            // per problem

@@ -245,6 +245,18 @@ qpb_status qpb_create_device(const qpb_problem* problem, const qpb_options* opti
   });
 }
 
+qpb_status qpb_reset(qpb_solver* solver, const qpb_problem* problems, size_t n_problems,
+                     uint64_t seed, const float* start) {
+  return guarded([&] {
+    require(solver != nullptr, "solver is NULL");
+    require(problems != nullptr && n_problems > 0, "no problems");
+    std::vector<qpb::ProblemView> views;
+    for (size_t q = 0; q < n_problems; ++q) views.push_back(made_problem(problems + q));
+    use_solver_device(solver);
+    solver->impl.reset(views, seed, reinterpret_cast<const float2*>(start));
+  });
+}
+
 qpb_status qpb_results_device(qpb_solver* solver, float* objects, uint8_t* supports,
                               float* errors) {
   return guarded([&] {

@@ -12,8 +12,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "device_setup.cuh"
 #include "fast_pass.cuh"
@@ -306,59 +311,13 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   options_.start = nullptr;
   amp_stride_ = problems_ > 1 ? n_ : 0;
 
-  // Per problem: FFT-order amplitude, mask, support; signed amplitude in the
-  // storage type (in the modulus pass's CTA order when that pass runs the
-  // register-resident kernel, so each CTA stages its tile with one bulk copy).
   const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
-  const int lines = fast_pass_lines(mod);
-  const bool tile = lines > 0 && mod.S > 1 && !resident_;
-  std::vector<float> amp_all;
-  std::vector<unsigned char> signed_all;
-  std::vector<std::vector<std::uint8_t>> supports;
-  const bool on_device = problem.on_device;
-  for (const ProblemView& q : problems) {
-    if (q.on_device != on_device) throw InvalidArgument("problems mix host and device arrays");
-  }
-  for (const ProblemView& q : (on_device ? std::vector<ProblemView>{} : problems)) {
-    const auto amp = host_roll(q.amplitude, d_, true);
-    std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
-    if (q.mask) {
-      mask = host_roll(q.mask, d_, true);
-      for (auto& m : mask) m = m != 0;
-    }
-    auto sup = host_roll(q.support, d_, true);
-    for (auto& v : sup) v = v != 0;
-    energies_.push_back(usable_energy(amp, mask));
-    auto bytes = signed_amplitude(amp, mask, options.amp_storage);
-    if (tile) {
-      const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
-      bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
-    }
-    amp_all.insert(amp_all.end(), amp.begin(), amp.end());
-    signed_all.insert(signed_all.end(), bytes.begin(), bytes.end());
-    supports.push_back(std::move(sup));
-  }
-  amp_tiled_ = tile;
+  amp_tiled_ = fast_pass_lines(mod) > 0 && mod.S > 1 && !resident_;
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
+  amp_ = DeviceBuffer<unsigned char>(static_cast<std::size_t>(problems_) * n_ * elem);
+  amp_f_ = DeviceBuffer<float>(static_cast<std::size_t>(problems_) * n_);
   support_ = DeviceBuffer<std::uint8_t>(total);
-  DeviceBuffer<float> amp_f;  // FP32 FFT-order amplitude of every problem, for the random starts
-  if (on_device) {
-    // The same preparation on the device, from the caller's device arrays.
-    const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
-    amp_f = DeviceBuffer<float>(static_cast<std::size_t>(problems_) * n_);
-    amp_ = DeviceBuffer<unsigned char>(static_cast<std::size_t>(problems_) * n_ * elem);
-    for (int q = 0; q < problems_; ++q) {
-      energies_.push_back(prepare_problem_device(
-          problems[q], d_, options.amp_storage, mod.L, mod.S, tile ? lines : 0,
-          amp_f.get() + static_cast<std::size_t>(q) * n_,
-          amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
-          support_.get() + static_cast<std::size_t>(q) * spp_ * n_, stream_));
-    }
-  } else {
-    amp_ = upload(signed_all, stream_);
-    amp_f = upload(amp_all, stream_);
-  }
-
   x_ = DeviceBuffer<float2>(total);
   w_ = DeviceBuffer<float2>(total);
   saved_ = DeviceBuffer<std::uint8_t>(total);
@@ -366,6 +325,77 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   moments_ = DeviceBuffer<unsigned long long>(2 * static_cast<std::size_t>(starts_));
   ctrl_ = DeviceBuffer<Ctrl>(1);
   counters_ = DeviceBuffer<int>(static_cast<std::size_t>(groups_));
+  load(problems, options.seed, options.start);
+}
+
+void Solver::reset(const std::vector<ProblemView>& problems, std::uint64_t seed,
+                   const float2* start) {
+  if (static_cast<int>(problems.size()) != problems_) {
+    throw InvalidArgument("reset needs as many problems as the solver was built for");
+  }
+  for (const ProblemView& q : problems) {
+    const Dims3 dq = dims_of(q);
+    if (q.ndim != ndim_ || dq.d0 != d_.d0 || dq.d1 != d_.d1 || dq.d2 != d_.d2) {
+      throw InvalidArgument("reset needs problems of the solver's shape");
+    }
+    if (!q.amplitude || !q.support) {
+      throw InvalidArgument("problem arrays do not match its shape; build it with make_problem");
+    }
+  }
+  load(problems, seed, start);
+}
+
+// Problems into the solver's buffers: per problem the FFT-order amplitude,
+// mask and support, the signed amplitude in the storage type (in the modulus
+// pass's CTA order when that pass runs the register-resident kernel, so each
+// CTA stages its tile with one bulk copy) and the usable energy; then the
+// starts, drawn or given. The captured graphs stay valid: every buffer keeps
+// its address.
+void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
+                  const float2* start) {
+  const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
+  const int lines = amp_tiled_ ? fast_pass_lines(mod) : 0;
+  const std::size_t elem = options_.amp_storage == AmpStorage::kF32 ? 4 : 2;
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  const bool on_device = problems[0].on_device;
+  for (const ProblemView& q : problems) {
+    if (q.on_device != on_device) throw InvalidArgument("problems mix host and device arrays");
+  }
+  energies_.clear();
+  std::vector<float> amp_all;
+  std::vector<unsigned char> signed_all;
+  std::vector<std::vector<std::uint8_t>> supports;
+  if (on_device) {
+    // The same preparation on the device, from the caller's device arrays.
+    for (int q = 0; q < problems_; ++q) {
+      energies_.push_back(prepare_problem_device(
+          problems[q], d_, options_.amp_storage, mod.L, mod.S, lines,
+          amp_f_.get() + static_cast<std::size_t>(q) * n_,
+          amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
+          support_.get() + static_cast<std::size_t>(q) * spp_ * n_, stream_));
+    }
+  } else {
+    for (const ProblemView& q : problems) {
+      const auto amp = host_roll(q.amplitude, d_, true);
+      std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
+      if (q.mask) {
+        mask = host_roll(q.mask, d_, true);
+        for (auto& m : mask) m = m != 0;
+      }
+      auto sup = host_roll(q.support, d_, true);
+      for (auto& v : sup) v = v != 0;
+      energies_.push_back(usable_energy(amp, mask));
+      auto bytes = signed_amplitude(amp, mask, options_.amp_storage);
+      if (lines > 0) bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
+      amp_all.insert(amp_all.end(), amp.begin(), amp.end());
+      signed_all.insert(signed_all.end(), bytes.begin(), bytes.end());
+      supports.push_back(std::move(sup));
+    }
+    QPB_CHECK(cudaMemcpyAsync(amp_.get(), signed_all.data(), signed_all.size(),
+                              cudaMemcpyHostToDevice, stream_));
+    QPB_CHECK(cudaMemcpyAsync(amp_f_.get(), amp_all.data(), amp_all.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, stream_));
+  }
   QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
   const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
@@ -383,10 +413,12 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   }
   stream_.sync();  // the host vectors above are released at the end of this scope
   errors_.assign(static_cast<std::size_t>(starts_), {});
+  iteration_ = 0;
+  run_iterations_ = 0;
 
-  if (options.start) {
+  if (start) {
     // Given starts, centre-origin: to FFT order, cut to the support (cpu_solver.cpp:37-41).
-    QPB_CHECK(cudaMemcpyAsync(w_.get(), options.start, total * sizeof(float2), cudaMemcpyDefault,
+    QPB_CHECK(cudaMemcpyAsync(w_.get(), start, total * sizeof(float2), cudaMemcpyDefault,
                               stream_));
     roll<float2>(w_.get(), x_.get(), d_, starts_, true, stream_);
     support_project(x_.get(), support_.get(), n_, starts_, stream_);
@@ -396,7 +428,7 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
     // Random phases on the measured amplitude, inverse transform, cut to the
     // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
     for (int g = 0; g < groups_; ++g) {
-      random_wave(w(g), amp_f.get(), amp_stride_, spp_, n_, batch_, options.seed,
+      random_wave(w(g), amp_f_.get(), amp_stride_, spp_, n_, batch_, seed,
                   static_cast<std::uint64_t>(g) * batch_, stream_);
       const int outer = runner_.outer();
       runner_.launch(Mode::kInv, outer, base(Mode::kInv, outer, g), stream_);
@@ -409,7 +441,6 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
       runner_.launch(Mode::kUpd, 2, u, stream_);
       if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
     }
-    stream_.sync();
     wave_valid_ = true;
   }
   stream_.sync();
@@ -769,19 +800,54 @@ void Solver::results_device(float2* objects, std::uint8_t* supports, float* erro
   }
 }
 
+namespace {
+
+// memcpy split over a few threads: one core does not saturate host memory.
+void parallel_copy(void* dst, const void* src, std::size_t bytes) {
+  constexpr std::size_t kChunk = 2u << 20;
+  const std::size_t parts =
+      std::min<std::size_t>(std::max<std::size_t>(bytes / kChunk, 1),
+                            std::max(1u, std::min(8u, std::thread::hardware_concurrency())));
+  if (parts <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const std::size_t step = (bytes + parts - 1) / parts;
+  std::vector<std::thread> workers;
+  for (std::size_t k = 1; k < parts; ++k) {
+    const std::size_t from = k * step;
+    if (from >= bytes) break;
+    workers.emplace_back([=] {
+      std::memcpy(static_cast<char*>(dst) + from, static_cast<const char*>(src) + from,
+                  std::min(step, bytes - from));
+    });
+  }
+  std::memcpy(dst, src, std::min(step, bytes));
+  for (auto& w : workers) w.join();
+}
+
+}  // namespace
+
 void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  // Device rolls to centre-origin, one copy each into page-locked staging,
+  // then into the caller's (pageable) arrays.
+  const std::size_t obj_bytes = objects ? total * sizeof(float2) : 0;
+  const std::size_t sup_bytes = supports ? total : 0;
+  unsigned char* staging = staging_.reserve(std::max<std::size_t>(obj_bytes + sup_bytes, 1));
   if (objects) {
     roll<float2>(x_.get(), w_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(objects, w_.get(), total * sizeof(float2), cudaMemcpyDeviceToHost,
-                              stream_));
+    QPB_CHECK(cudaMemcpyAsync(staging, w_.get(), obj_bytes, cudaMemcpyDeviceToHost, stream_));
     wave_valid_ = false;
   }
   if (supports) {
     roll<std::uint8_t>(support_.get(), saved_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(supports, saved_.get(), total, cudaMemcpyDeviceToHost, stream_));
+    QPB_CHECK(cudaMemcpyAsync(staging + obj_bytes, saved_.get(), sup_bytes, cudaMemcpyDeviceToHost,
+                              stream_));
   }
   stream_.sync();
+  if (objects) parallel_copy(objects, staging, obj_bytes);
+  if (supports) parallel_copy(supports, staging + obj_bytes, sup_bytes);
   if (errors) {
     const std::size_t count = error_count();
     for (int s = 0; s < starts_; ++s) {
@@ -793,13 +859,27 @@ void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
 // ------------------------------------------------------------------- operators
 namespace {
 
+// Line plans (device twiddle tables) of the single operators, kept per device
+// for the process so that repeated calls allocate nothing for them.
+PlanCache& operator_plans() {
+  static std::mutex mutex;
+  static std::map<int, std::unique_ptr<PlanCache>> per_device;
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  auto& slot = per_device[device];
+  if (!slot) slot = std::make_unique<PlanCache>();
+  return *slot;
+}
+
 struct OperatorContext {
   Dims3 d;
   int ndim;
-  PlanCache plans;
+  PlanCache& plans;
   Stream stream;
   PassRunner runner;
-  OperatorContext(Dims3 dims, int nd) : d(dims), ndim(nd), runner(dims, nd, plans) {}
+  OperatorContext(Dims3 dims, int nd)
+      : d(dims), ndim(nd), plans(operator_plans()), runner(dims, nd, plans) {}
 };
 
 ProblemView view_of(int ndim, const long long* shape) {

@@ -51,6 +51,32 @@ class DeviceBuffer {
   std::size_t count_ = 0;
 };
 
+// Owning page-locked host allocation (the staging area of device-to-host copies).
+class PinnedBuffer {
+ public:
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() {
+    if (ptr_) cudaFreeHost(ptr_);
+  }
+  // At least `bytes`, reallocated only to grow.
+  unsigned char* reserve(std::size_t bytes) {
+    if (bytes > bytes_) {
+      if (ptr_) cudaFreeHost(ptr_);
+      ptr_ = nullptr;
+      bytes_ = 0;
+      QPB_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&ptr_), bytes, cudaHostAllocDefault));
+      bytes_ = bytes;
+    }
+    return ptr_;
+  }
+
+ private:
+  unsigned char* ptr_ = nullptr;
+  std::size_t bytes_ = 0;
+};
+
 // A stream the object creates (and destroys), or one the caller lends.
 class Stream {
  public:
@@ -205,6 +231,10 @@ class Solver {
   Solver& operator=(const Solver&) = delete;
 
   void run(const OpDesc* ops, std::size_t count);
+  // New problems of the same shape and count in the same solver: buffers and
+  // captured graphs are kept, the iterate, supports and error histories start
+  // afresh from `seed` or the given starts (as construction does).
+  void reset(const std::vector<ProblemView>& problems, std::uint64_t seed, const float2* start);
   std::size_t error_count() const { return errors_.empty() ? 0 : errors_[0].size(); }
   int starts() const { return starts_; }
   int problems() const { return problems_; }
@@ -252,6 +282,7 @@ class Solver {
   }
   PassParams base(Mode mode, int axis3, int g) const;
 
+  void load(const std::vector<ProblemView>& problems, std::uint64_t seed, const float2* start);
   void enqueue_iteration(int g, cudaStream_t s);
   void enqueue_chunk(int len, cudaStream_t s);  // resident: `len` iterations in one launch
   void enqueue_establish(int g);
@@ -280,6 +311,8 @@ class Solver {
   std::vector<double> energies_;     // usable energy per problem
   long long amp_stride_ = 0;         // elements between problems' amplitudes in amp_
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
+  DeviceBuffer<float> amp_f_;        // FP32 FFT-order amplitude, for the random starts
+  PinnedBuffer staging_;             // results() copies through it
   bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
   bool resident_ = false;            // iterations run by the resident kernel
   DeviceBuffer<float2> x_;

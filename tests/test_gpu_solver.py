@@ -229,3 +229,46 @@ def test_negative_intensity_warns(gpu, readme):
     _, support, intensity = readme
     with pytest.warns(UserWarning, match="negative"):
         qpc.reconstruct(intensity - 0.5 * intensity.max(), support=support, recipe=Recipe(ER(1)))
+
+
+@pytest.mark.parametrize("schedule", ["streamed", "resident"])
+def test_reset_equals_a_fresh_solver(gpu, schedule):
+    """Solver.reset keeps buffers and graphs; the next problem's results are
+    those of a solver built for it."""
+    _, s1, i1 = triangle((64, 64), 20)
+    _, s2, i2 = triangle((64, 64), 14)
+    p1 = qpc.make_problem(i1, support=s1)
+    p2 = qpc.make_problem(i2, support=s2)
+    recipe = Recipe(HIO(12), Shrinkwrap(), ER(8))
+    with qpc.Solver(p1, starts=4, seed=1, sync_every=5, schedule=schedule) as s:
+        s.run(recipe)
+        s.reset(p2, seed=7)
+        s.run(recipe)
+        reused = s.results()
+        with pytest.raises(ValueError, match="shape"):
+            s.reset(qpc.make_problem(np.pad(i2, 2)), seed=1)
+    with qpc.Solver(p2, starts=4, seed=7, sync_every=5, schedule=schedule) as s:
+        s.run(recipe)
+        fresh = s.results()
+    for a, b in zip(reused, fresh, strict=True):
+        np.testing.assert_array_equal(a.object, b.object)
+        np.testing.assert_array_equal(a.support, b.support)
+        np.testing.assert_allclose(a.errors, b.errors, rtol=1e-6)
+
+
+def test_reconstruct_reuses_its_solver(gpu):
+    """Two reconstruct() calls of one shape: the second loads into the first's
+    solver and gives what a fresh solver gives."""
+    _, s1, i1 = triangle((48, 40), 12)
+    _, s2, i2 = triangle((48, 40), 10)
+    recipe = Recipe(RAAR(10), ER(5))
+    qpc.api.clear_cache()
+    a = qpc.reconstruct(i1, support=s1, recipe=recipe, starts=2, seed=3)
+    b = qpc.reconstruct(i2, support=s2, recipe=recipe, starts=2, seed=3)
+    with qpc.Solver(qpc.make_problem(i2, support=s2), starts=2, seed=3) as s:
+        s.run(recipe)
+        fresh = s.results()
+    for x, y in zip(b, fresh, strict=True):
+        np.testing.assert_array_equal(x.object, y.object)
+    assert not np.array_equal(a[0].object, b[0].object)
+    qpc.api.clear_cache()
