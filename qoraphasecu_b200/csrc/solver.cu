@@ -17,7 +17,6 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "device_setup.cuh"
@@ -800,54 +799,19 @@ void Solver::results_device(float2* objects, std::uint8_t* supports, float* erro
   }
 }
 
-namespace {
-
-// memcpy split over a few threads: one core does not saturate host memory.
-void parallel_copy(void* dst, const void* src, std::size_t bytes) {
-  constexpr std::size_t kChunk = 2u << 20;
-  const std::size_t parts =
-      std::min<std::size_t>(std::max<std::size_t>(bytes / kChunk, 1),
-                            std::max(1u, std::min(8u, std::thread::hardware_concurrency())));
-  if (parts <= 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  const std::size_t step = (bytes + parts - 1) / parts;
-  std::vector<std::thread> workers;
-  for (std::size_t k = 1; k < parts; ++k) {
-    const std::size_t from = k * step;
-    if (from >= bytes) break;
-    workers.emplace_back([=] {
-      std::memcpy(static_cast<char*>(dst) + from, static_cast<const char*>(src) + from,
-                  std::min(step, bytes - from));
-    });
-  }
-  std::memcpy(dst, src, std::min(step, bytes));
-  for (auto& w : workers) w.join();
-}
-
-}  // namespace
-
 void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
-  // Device rolls to centre-origin, one copy each into page-locked staging,
-  // then into the caller's (pageable) arrays.
-  const std::size_t obj_bytes = objects ? total * sizeof(float2) : 0;
-  const std::size_t sup_bytes = supports ? total : 0;
-  unsigned char* staging = staging_.reserve(std::max<std::size_t>(obj_bytes + sup_bytes, 1));
   if (objects) {
     roll<float2>(x_.get(), w_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(staging, w_.get(), obj_bytes, cudaMemcpyDeviceToHost, stream_));
+    QPB_CHECK(cudaMemcpyAsync(objects, w_.get(), total * sizeof(float2), cudaMemcpyDeviceToHost,
+                              stream_));
     wave_valid_ = false;
   }
   if (supports) {
     roll<std::uint8_t>(support_.get(), saved_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(staging + obj_bytes, saved_.get(), sup_bytes, cudaMemcpyDeviceToHost,
-                              stream_));
+    QPB_CHECK(cudaMemcpyAsync(supports, saved_.get(), total, cudaMemcpyDeviceToHost, stream_));
   }
   stream_.sync();
-  if (objects) parallel_copy(objects, staging, obj_bytes);
-  if (supports) parallel_copy(supports, staging + obj_bytes, sup_bytes);
   if (errors) {
     const std::size_t count = error_count();
     for (int s = 0; s < starts_; ++s) {

@@ -51,32 +51,6 @@ class DeviceBuffer {
   std::size_t count_ = 0;
 };
 
-// Owning page-locked host allocation (the staging area of device-to-host copies).
-class PinnedBuffer {
- public:
-  PinnedBuffer() = default;
-  PinnedBuffer(const PinnedBuffer&) = delete;
-  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
-  ~PinnedBuffer() {
-    if (ptr_) cudaFreeHost(ptr_);
-  }
-  // At least `bytes`, reallocated only to grow.
-  unsigned char* reserve(std::size_t bytes) {
-    if (bytes > bytes_) {
-      if (ptr_) cudaFreeHost(ptr_);
-      ptr_ = nullptr;
-      bytes_ = 0;
-      QPB_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&ptr_), bytes, cudaHostAllocDefault));
-      bytes_ = bytes;
-    }
-    return ptr_;
-  }
-
- private:
-  unsigned char* ptr_ = nullptr;
-  std::size_t bytes_ = 0;
-};
-
 // A stream the object creates (and destroys), or one the caller lends.
 class Stream {
  public:
@@ -312,7 +286,6 @@ class Solver {
   long long amp_stride_ = 0;         // elements between problems' amplitudes in amp_
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
   DeviceBuffer<float> amp_f_;        // FP32 FFT-order amplitude, for the random starts
-  PinnedBuffer staging_;             // results() copies through it
   bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
   bool resident_ = false;            // iterations run by the resident kernel
   DeviceBuffer<float2> x_;
