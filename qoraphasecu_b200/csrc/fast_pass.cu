@@ -38,16 +38,17 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 // and support tiles of a row update); then two mbarriers (16 bytes).
 // CTA shape of a streamed pass: lines per CTA, threads, the CTAs per SM the
 // register budget is sized for (registers <= 64K / (NT * MIN_CTAS)) and the
-// exchange rows. Rows of 256 points use 8 lines per CTA (128 threads, up to 6
-// CTAs per SM), which halves a launch's last partial wave; their columns keep
-// 16, whose 128-byte row segments load better.
+// exchange rows. Rows of 256 points use 4 lines per CTA (64 threads, up to 12
+// CTAs per SM), which shortens a launch's last partial wave; their columns
+// keep 16, whose 128-byte row segments load better (fewer columns per CTA
+// measured slower).
 template <int L, bool ROWS>
 struct Tiling {
   using G = Geometry<L>;
   static constexpr int LINES =
-      (ROWS && L == 256) ? 8 : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
+      (ROWS && L == 256) ? 4 : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
   static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 128 ? 6 : (NT <= 256 ? 3 : 1);
+  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 6 : (NT <= 256 ? 3 : 1));
   static constexpr int SMEM = G::STAGES > 1 ? LINES * G::PITCH * 8 : 0;
 };
 
