@@ -272,3 +272,16 @@ def test_reconstruct_reuses_its_solver(gpu):
         np.testing.assert_array_equal(x.object, y.object)
     assert not np.array_equal(a[0].object, b[0].object)
     qpc.api.clear_cache()
+
+
+@pytest.mark.parametrize("shape,m", [((6, 32, 32), 4), ((8, 64, 64), 6), ((4, 128, 128), 4)])
+def test_3d_register_passes_match_fp64(gpu, shape, m):
+    """3D iterations through the register-resident passes on every axis
+    (slices of side 32, 64, 128; z extents 4..8)."""
+    _, support, intensity = triangle(shape, m)
+    recipe = Recipe(HIO(8), Shrinkwrap(), RAAR(6), ER(6))
+    ref, ours = run_both(intensity, support, recipe, starts=2, seed=5, sync_every=4)
+    for (r_obj, r_sup, r_err), run in zip(ref, ours, strict=True):
+        np.testing.assert_allclose(run.errors, r_err, rtol=1e-4, atol=1e-7)
+        assert fp64.relative_diff(run.object, r_obj) < 1e-4
+        np.testing.assert_array_equal(run.support, r_sup)
