@@ -39,16 +39,25 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 // CTA shape of a streamed pass: lines per CTA, threads, the CTAs per SM the
 // register budget is sized for (registers <= 64K / (NT * MIN_CTAS)) and the
 // exchange rows. Rows of 256 points use 4 lines per CTA (64 threads, up to 12
-// CTAs per SM), which shortens a launch's last partial wave; their columns
-// keep 16, whose 128-byte row segments load better (fewer columns per CTA
-// measured slower).
+// CTAs per SM), which shortens a launch's last partial wave, and rows of 128
+// use 8 (64 threads; the 128^3 x-axis update pass measured 60.5 us against
+// 69.6 us with 32 lines and 62.6 us with 4). Rows of 512 and 1024 points take
+// one line per CTA, budgeted 128 registers a thread (their three-stage
+// transforms spill at 80): a 512^2 update pass of 16 starts measured 29.6 us
+// against 39.4 us with 16 lines per CTA and 30.8 us with 2. Columns keep
+// 256 / T lines up to 256 points (16 at 256, and at 512), whose 128-byte and
+// longer row segments load better (fewer columns per CTA measured slower: 8
+// at 512 took 37.2 us against 35.2 us).
 template <int L, bool ROWS>
 struct Tiling {
   using G = Geometry<L>;
-  static constexpr int LINES =
-      (ROWS && L == 256) ? 4 : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
+  static constexpr int LINES = (ROWS && L >= 512)   ? 1
+                               : (ROWS && L == 256) ? 4
+                               : (ROWS && L == 128) ? 8
+                                                    : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
   static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 6 : (NT <= 256 ? 3 : 1));
+  static constexpr int MIN_CTAS = L >= 512 ? (NT < 512 ? 512 / NT : 1)
+                                           : (NT <= 64 ? 12 : (NT <= 128 ? 6 : (NT <= 256 ? 3 : 1)));
   static constexpr int SMEM = G::STAGES > 1 ? LINES * G::PITCH * 8 : 0;
 };
 

@@ -53,7 +53,7 @@ def beamstop(shape, radius):
 
 
 def square(n=64, seed=0, ndim=2):
-    """Config-1 object: uniform amplitude and phase inside a centred square."""
+    """Square object: uniform amplitude and phase inside a centred square."""
     rng = np.random.default_rng(seed)
     m = max(1, round(24 * n / 64))
     shape = (n,) * ndim
@@ -67,7 +67,7 @@ def square(n=64, seed=0, ndim=2):
 
 
 def gaussians(n=256, seed=1000, peak=1e6, stop=8.0):
-    """Config-2 problem: returns (object, intensity, mask)."""
+    """Five Gaussian blobs with a smooth phase, Poisson counts, beamstop: returns (object, intensity, mask)."""
     rng = np.random.default_rng(seed)
     y, x = centred_coords((n, n))
     scale = n / 256
@@ -95,7 +95,7 @@ def gaussians_recipe() -> Recipe:
 
 
 def uneven_batch(count=64, seed=2000, sizes=(64, 128, 256, 512), peak=1e6):
-    """Config-3 problems: sides uniform over ``sizes``, square objects, beamstop n/32."""
+    """Uneven batch: sides uniform over ``sizes``, square objects, beamstop n/32."""
     rng = np.random.default_rng(seed)
     problems = []
     for k in range(count):
@@ -112,7 +112,7 @@ def uneven_recipe() -> Recipe:
 
 
 def crystal(n=128, seed=3000, peak=1e7):
-    """Config-5 3D Bragg-like object: returns (object, intensity)."""
+    """3D Bragg-like crystal object: returns (object, intensity)."""
     rng = np.random.default_rng(seed)
     z, y, x = centred_coords((n, n, n))
     scale = n / 128
