@@ -129,14 +129,15 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference arm
-def reference_sample(problem_arrays, starts, iterations, threads):
+def reference_sample(problem_arrays, starts, iterations, threads, port=False):
     """Times `iterations` RAAR iterations of `starts` starts on the host CPU with
-    the reference's own CpuSolver (compiled from its sources) when available,
-    else the oracle's numpy/pocketfft port. Returns (seconds, kind, label)."""
+    the reference's own CpuSolver (compiled from its sources) when available
+    and `port` is false, else the oracle's numpy port of CpuSolver::iterate on
+    scipy.fft (pocketfft C++). Returns (seconds, kind, label)."""
     intensity, mask = problem_arrays
     from oracle import ref as oracle_ref
 
-    if oracle_ref.available():
+    if not port and oracle_ref.available():
         seconds = oracle_ref.time_iterations(intensity, mask, starts, iterations, threads)
         return seconds, "reference", "QoraPhaseCU CpuSolver (OpenMP loops, project FFT shim)"
     import numpy as np
@@ -150,13 +151,13 @@ def reference_sample(problem_arrays, starts, iterations, threads):
     return time.perf_counter() - t0, "port", "numpy port of CpuSolver::iterate, scipy.fft (pocketfft)"
 
 
-def cpu_baseline(intensity, mask, budget_s=10.0):
+def cpu_baseline(intensity, mask, budget_s=10.0, port=False):
     threads = len(os.sched_getaffinity(0))
     iters = 2
-    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads)
+    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads, port)
     # grow the sample to about `budget_s` of CPU work
     iters = max(2, min(200, int(iters * budget_s / max(seconds, 1e-3))))
-    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads)
+    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads, port)
     return {
         "value": STARTS * iters / seconds,
         "unit": UNIT,
@@ -629,6 +630,11 @@ def main(argv=None):
     line["clocks"] = clocks.summary()
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(intensity, mask, budget_s=args.cpu_seconds)
+        if line["cpu_baseline"]["kind"] == "reference":
+            # the second CPU figure: the same iteration on pocketfft (scipy.fft),
+            # the FFT the reference's CPU backend links
+            line["cpu_baseline_pocketfft"] = cpu_baseline(intensity, mask,
+                                                          budget_s=args.cpu_seconds, port=True)
     solver.close()
     if dist:
         dist.barrier()
