@@ -227,7 +227,12 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   }
 
   constexpr bool kStartsInverse = M == Mode::kInv || M == Mode::kUpd;
-  transform<L, kStartsInverse, kWarpLocal>(v, t, tw, row);
+  // The last exchange's closing barrier is needed only before a second
+  // transform with no block barrier in between (the blur's); a modulus pass
+  // passes one in its error sum, an update in its store, and the passes of a
+  // single transform only write the row again after the barrier below.
+  constexpr bool kTrail = M == Mode::kBlur || M == Mode::kBlurMag;
+  transform<L, kStartsInverse, kWarpLocal, kTrail>(v, t, tw, row);
 
   if constexpr (St::kAmp) {
     if (!staged(bar)) return;
@@ -243,9 +248,11 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * Ti::LINES + l]);
       v[m] = pointwise_projection<M>(v[m], a, s, acc);
     }
-    const double total = block_sum_double(static_cast<double>(acc));
+    // one call per CTA; its first barrier also orders the forward transform's
+    // exchange reads before the inverse's writes
+    const double total = block_sum_double<false>(static_cast<double>(acc));
     if (tid == 0 && err_slot) atomicAdd(err_slot, total);
-    transform<L, true, kWarpLocal>(v, t, tw, row);
+    transform<L, true, kWarpLocal, false>(v, t, tw, row);
   } else if constexpr (M == Mode::kUpd) {
     if constexpr (St::kUpd) {
       if (!staged(side_bar)) return;
@@ -284,7 +291,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       __syncthreads();
     }
     if (p.bump_counter && blockIdx.x == 0 && tid == 0) ++p.ctrl->counters[p.group];
-    transform<L, false, kWarpLocal>(v, t, tw, row);
+    transform<L, false, kWarpLocal, false>(v, t, tw, row);
   } else if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
     const float inv_l = 1.0f / static_cast<float>(L);
 #pragma unroll
@@ -293,13 +300,13 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       const float f = fftfreq(static_cast<std::uint32_t>(j), static_cast<std::uint32_t>(L));
       v[m] = cscale(v[m], expf(p.blur_k * f * f) * inv_l);
     }
-    transform<L, true, kWarpLocal>(v, t, tw, row);
+    transform<L, true, kWarpLocal, false>(v, t, tw, row);
   }
 
   if constexpr (St::kRowTma) {
     // Region W is free once every warp is past its last exchange: the output
     // tile goes there and leaves by one bulk store.
-    if constexpr (kWarpLocal) __syncthreads();
+    __syncthreads();
 #pragma unroll
     for (int m = 0; m < E; ++m) wtile[l * L + t + T * m] = v[m];
     fence_proxy_async();

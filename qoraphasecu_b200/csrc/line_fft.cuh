@@ -62,8 +62,10 @@ __device__ __forceinline__ void line_sync() {
 
 // One Stockham stage of radix R over the thread's E registers. NS is the
 // product of the radices before it; LAST stages leave values in place,
-// others exchange through the line's shared-memory row.
-template <int L, int R, int NS, bool LAST, bool INV, bool WARP_LOCAL = false>
+// others exchange through the line's shared-memory row. TRAIL orders the
+// exchange's reads before any later write of the row; a caller may drop it
+// when a block barrier separates them anyway.
+template <int L, int R, int NS, bool LAST, bool INV, bool WARP_LOCAL = false, bool TRAIL = true>
 __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
                                       const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
@@ -99,15 +101,18 @@ __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
     line_sync<WARP_LOCAL>();
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = row[swz(t + T * m)];
-    line_sync<WARP_LOCAL>();
+    if constexpr (TRAIL) line_sync<WARP_LOCAL>();
   }
 }
 
 // Forward (INV false) or inverse unnormalised transform of the line held in
 // v. With WARP_LOCAL the caller guarantees that the line's threads share a
 // warp (T <= 32, lines not straddling warps) and that no other warp touches
-// `row` during the call; then only warp barriers separate the stages.
-template <int L, bool INV, bool WARP_LOCAL = false>
+// `row` during the call; then only warp barriers separate the stages. With
+// TRAIL false the transform returns without the barrier after its last
+// exchange: the caller must pass a block barrier before anything writes the
+// row again.
+template <int L, bool INV, bool WARP_LOCAL = false, bool TRAIL = true>
 __device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
                                           const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
@@ -115,11 +120,11 @@ __device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
   if constexpr (G::STAGES == 1) {
     stage<L, G::R0, 1, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else if constexpr (G::STAGES == 2) {
-    stage<L, G::R0, 1, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
     stage<L, G::R1, G::R0, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else {
     stage<L, G::R0, 1, false, INV, WARP_LOCAL>(v, t, tw, row);
-    stage<L, G::R1, G::R0, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R1, G::R0, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
     stage<L, G::R2, G::R0 * G::R1, true, INV, WARP_LOCAL>(v, t, tw, row);
   }
 }

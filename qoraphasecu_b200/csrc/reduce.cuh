@@ -18,7 +18,10 @@ __device__ __forceinline__ double warp_sum_double(double v) {
 }
 
 // Sum over the block, valid in thread 0. Every thread of the block must call
-// it; blockDim.x is a multiple of 32 and at most 1024.
+// it; blockDim.x is a multiple of 32 and at most 1024. AGAIN keeps the closing
+// barrier that a second call in the same block needs; either way the call
+// holds one block barrier after every thread has entered it.
+template <bool AGAIN = true>
 __device__ __forceinline__ double block_sum_double(double v) {
   __shared__ double partial[32];
   v = warp_sum_double(v);
@@ -30,7 +33,7 @@ __device__ __forceinline__ double block_sum_double(double v) {
     v = lane < static_cast<int>(blockDim.x >> 5) ? partial[lane] : 0.0;
     v = warp_sum_double(v);
   }
-  __syncthreads();
+  if constexpr (AGAIN) __syncthreads();
   return v;
 }
 
