@@ -620,8 +620,12 @@ def main(argv=None):
         line["e2e"] = {
             "value": world * STARTS * iters / e2e_s,
             "unit": UNIT,
-            "h2d_bytes_per_step": int(n * (4 + 8 + 4 + 1 + 4)),
-            "d2h_bytes_per_step": int(n * 8 + STARTS * n * (8 + 1) + STARTS * iters * 8),
+            # up: the intensity for the autocorrelation support (4 B), then the
+            # amplitude, mask and support the solver prepares on the device
+            # (4 + 1 + 1 B); down: the support (1 B), every start's object and
+            # support (8 + 1 B) and its FP64 error history
+            "h2d_bytes_per_step": int(n * (4 + 4 + 1 + 1)),
+            "d2h_bytes_per_step": int(n * 1 + STARTS * n * (8 + 1) + STARTS * iters * 8),
             "seconds_per_step": e2e_s,
             "path": "qoraphasecu_b200.reconstruct (make_problem + solver + results)",
         }

@@ -9,6 +9,7 @@ Mirrors the reference's ``python/qoraphasecu/api.py`` (``reconstruct`` at
 from __future__ import annotations
 
 import ctypes
+import sys
 import threading
 import warnings
 from dataclasses import dataclass
@@ -280,6 +281,19 @@ def make_problem(intensity, support=None, mask=None, support_threshold: float = 
     return Problem(amp, m, s)
 
 
+def _host_empty(shape, dtype):
+    """A host array for results the device writes: page-locked memory from
+    torch's caching pinned-memory allocator when torch is already loaded (the
+    copy runs at full link speed, and a block the caller has dropped is reused
+    without a new page-locking call), else ordinary numpy memory."""
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available():
+        count = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        block = torch.empty(count, dtype=torch.uint8, pin_memory=True)
+        return block.numpy().view(dtype).reshape(shape)
+    return np.empty(shape, dtype)
+
+
 def _flag(name, array, shape):
     if array is None:
         return None
@@ -450,13 +464,13 @@ class Solver:
             return self._results_device()
         starts = self.starts
         count = self.error_count()
-        objects = np.empty((starts, *self.shape), np.complex64)
-        supports = np.empty((starts, *self.shape), np.uint8)
+        objects = _host_empty((starts, *self.shape), np.complex64)
+        supports = _host_empty((starts, *self.shape), np.uint8)
         errors = np.empty((starts, count), np.float32)
         _lib.check(self._lib.qpb_results(self._handle, _lib.ptr(objects), _lib.ptr(supports),
                                          _lib.ptr(errors)))
-        return [Reconstruction(objects[s], supports[s].astype(bool), errors[s])
-                for s in range(starts)]
+        supports = supports.view(np.bool_)  # the device writes 0 or 1
+        return [Reconstruction(objects[s], supports[s], errors[s]) for s in range(starts)]
 
     def _results_device(self):
         """Objects and supports as CUDA torch tensors, written by the device."""
@@ -560,16 +574,17 @@ class BatchSolver:
         count = self.error_count()
         sizes = [int(np.prod(p.shape)) for p in self.problems]
         total = self._starts * sum(sizes)
-        objects = np.empty(total, np.complex64)
-        supports = np.empty(total, np.uint8)
+        objects = _host_empty(total, np.complex64)
+        supports = _host_empty(total, np.uint8)
         errors = np.empty((len(self.problems), self._starts, count), np.float32)
         _lib.check(self._lib.qpb_results(self._handle, _lib.ptr(objects), _lib.ptr(supports),
                                          _lib.ptr(errors)))
+        supports = supports.view(np.bool_)  # the device writes 0 or 1
         out, at = [], 0
         for q, p in enumerate(self.problems):
             block = self._starts * sizes[q]
             obj = objects[at:at + block].reshape(self._starts, *p.shape)
-            sup = supports[at:at + block].reshape(self._starts, *p.shape).astype(bool)
+            sup = supports[at:at + block].reshape(self._starts, *p.shape)
             out.append([Reconstruction(obj[s], sup[s], errors[q, s]) for s in range(self._starts)])
             at += block
         return out

@@ -146,7 +146,7 @@ qpb_status qpb_make_problem(const float* intensity, int ndim, const int64_t* sha
     if (support) {
       for (long long i = 0; i < n; ++i) support_out[i] = support[i] != 0;
     } else {
-      qpb::autocorrelation_support(intensity, ndim, sh, support_threshold, support_out);
+      qpb::autocorrelation_support_host(intensity, ndim, sh, support_threshold, support_out);
     }
     for (long long i = 0; i < n; ++i) {
       amplitude_out[i] = std::sqrt(std::max(intensity[i], 0.0f));
@@ -162,7 +162,7 @@ qpb_status qpb_autocorrelation_support(const float* intensity, int ndim, const i
     require(intensity && out, "NULL array");
     long long sh[3] = {0, 0, 0};
     for (int a = 0; a < ndim; ++a) sh[a] = shape[a];
-    qpb::autocorrelation_support(intensity, ndim, sh, threshold, out);
+    qpb::autocorrelation_support_host(intensity, ndim, sh, threshold, out);
   });
 }
 

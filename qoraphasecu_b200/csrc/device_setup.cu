@@ -10,6 +10,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 
 #include "device_setup.cuh"
@@ -111,10 +114,15 @@ __global__ void nonzero_kernel(std::uint8_t* v, long long n) {
   QPB_LOOP(i, n) v[i] = v[i] != 0;
 }
 
-__global__ void energy_kernel(const float* amp, const std::uint8_t* mask, long long n, double* out) {
-  __shared__ double partial[kThreads / 32];
+// Usable energy, one block of kEnergyThreads: every element's share is added
+// in the same order on every call.
+constexpr int kEnergyThreads = 1024;
+
+__global__ void __launch_bounds__(kEnergyThreads)
+    energy_kernel(const float* amp, const std::uint8_t* mask, long long n, double* out) {
+  __shared__ double partial[kEnergyThreads / 32];
   double e = 0.0;
-  QPB_LOOP(i, n) {
+  for (long long i = threadIdx.x; i < n; i += kEnergyThreads) {
     if (!mask[i]) e += static_cast<double>(amp[i]) * amp[i];
   }
   for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
@@ -122,9 +130,76 @@ __global__ void energy_kernel(const float* amp, const std::uint8_t* mask, long l
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) t += partial[w];
-    atomicAdd(out, t);
+    for (int w = 0; w < kEnergyThreads / 32; ++w) t += partial[w];
+    *out = t;
   }
+}
+
+constexpr std::size_t align256(std::size_t bytes) { return (bytes + 255) / 256 * 256; }
+
+// Device memory for problem set-up, one arena per device, grown on demand and
+// kept for the process; set-up calls on one device take turns on it.
+struct SetupArena {
+  std::mutex mutex;
+  std::unique_ptr<Stream> stream;
+  DeviceBuffer<unsigned char> bytes;
+  unsigned char* reserve(std::size_t count) {
+    if (bytes.size() < count) {
+      bytes = DeviceBuffer<unsigned char>();
+      bytes = DeviceBuffer<unsigned char>(count);
+    }
+    return bytes.get();
+  }
+};
+
+SetupArena& setup_arena() {
+  static std::mutex mutex;
+  static auto* arenas = new std::map<int, std::unique_ptr<SetupArena>>();  // never freed
+  int device = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mutex);
+  auto& slot = (*arenas)[device];
+  if (!slot) {
+    slot = std::make_unique<SetupArena>();
+    slot->stream = std::make_unique<Stream>();
+  }
+  return *slot;
+}
+
+std::size_t support_scratch_bytes(long long n) {
+  const auto count = static_cast<std::size_t>(n);
+  return 256 + 2 * align256(count * sizeof(float)) + align256(count * sizeof(float2));
+}
+
+// The autocorrelation support of a centre-origin device intensity into `out`
+// (device): |IFFT(I)| in FFT order, centre-origin again, > threshold * max.
+// `scratch`: support_scratch_bytes(n) device bytes.
+void support_device(const float* intensity, Dims3 d, int ndim, float threshold, std::uint8_t* out,
+                    unsigned char* scratch, cudaStream_t stream) {
+  const long long n = d.n();
+  const std::size_t plane = align256(static_cast<std::size_t>(n) * sizeof(float));
+  auto* max_bits = reinterpret_cast<unsigned*>(scratch);
+  auto* ordered = reinterpret_cast<float*>(scratch + 256);
+  auto* mag = reinterpret_cast<float*>(scratch + 256 + plane);
+  auto* w = reinterpret_cast<float2*>(scratch + 256 + 2 * plane);
+  PassRunner runner(d, ndim, operator_plans());
+  QPB_CHECK(cudaMemsetAsync(max_bits, 0, sizeof(unsigned), stream));
+  roll<float>(intensity, ordered, d, 1, true, stream);
+  to_complex_kernel<<<blocks_for(n), kThreads, 0, stream>>>(ordered, w, n);
+  QPB_CHECK(cudaGetLastError());
+  for (int axis3 = runner.outer(); axis3 < 3; ++axis3) {
+    PassParams p = runner.params(Mode::kInv, axis3, 1);
+    p.w = w;
+    p.x = w;
+    runner.launch(Mode::kInv, axis3, p, stream);
+  }
+  magnitude_kernel<<<blocks_for(n), kThreads, 0, stream>>>(
+      w, ordered, n, 1.0f / std::sqrt(static_cast<float>(n)), max_bits);
+  QPB_CHECK(cudaGetLastError());
+  roll<float>(ordered, mag, d, 1, false, stream);
+  threshold_kernel<<<blocks_for(n), kThreads, 0, stream>>>(mag, n, max_bits, threshold, out);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(3);
 }
 
 }  // namespace
@@ -138,42 +213,18 @@ void make_problem_device(const float* intensity, int ndim, const long long* shap
   for (int a = 0; a < ndim && a < 3; ++a) v.shape[a] = shape[a];
   const Dims3 d = dims_of(v);
   const long long n = d.n();
-  DeviceBuffer<unsigned long long> flags(2);
-  QPB_CHECK(cudaMemsetAsync(flags.get(), 0, 2 * sizeof(unsigned long long), stream));
+  SetupArena& arena = setup_arena();
+  std::lock_guard<std::mutex> lock(arena.mutex);
+  unsigned char* scratch = arena.reserve(256 + (support ? 0 : support_scratch_bytes(n)));
+  auto* flags = reinterpret_cast<unsigned long long*>(scratch);
+  QPB_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned long long), stream));
   prepare_kernel<<<blocks_for(n), kThreads, 0, stream>>>(intensity, mask, support, n, amplitude_out,
-                                                          mask_out, support_out, flags.get());
+                                                          mask_out, support_out, flags);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
-  // Without a support: |IFFT(I)| in FFT order, centre-origin again, > threshold * max.
-  PlanCache plans;
-  DeviceBuffer<float> ordered(support ? 0 : static_cast<std::size_t>(n));
-  DeviceBuffer<float> mag(support ? 0 : static_cast<std::size_t>(n));
-  DeviceBuffer<float2> w(support ? 0 : static_cast<std::size_t>(n));
-  DeviceBuffer<unsigned> max_bits(1);
-  if (!support) {
-    PassRunner runner(d, ndim, plans);
-    QPB_CHECK(cudaMemsetAsync(max_bits.get(), 0, sizeof(unsigned), stream));
-    roll<float>(intensity, ordered.get(), d, 1, true, stream);
-    to_complex_kernel<<<blocks_for(n), kThreads, 0, stream>>>(ordered.get(), w.get(), n);
-    QPB_CHECK(cudaGetLastError());
-    for (int axis3 = runner.outer(); axis3 < 3; ++axis3) {
-      PassParams p = runner.params(Mode::kInv, axis3, 1);
-      p.w = w.get();
-      p.x = w.get();
-      runner.launch(Mode::kInv, axis3, p, stream);
-    }
-    magnitude_kernel<<<blocks_for(n), kThreads, 0, stream>>>(
-        w.get(), ordered.get(), n, 1.0f / std::sqrt(static_cast<float>(n)), max_bits.get());
-    QPB_CHECK(cudaGetLastError());
-    roll<float>(ordered.get(), mag.get(), d, 1, false, stream);
-    threshold_kernel<<<blocks_for(n), kThreads, 0, stream>>>(mag.get(), n, max_bits.get(),
-                                                             support_threshold, support_out);
-    QPB_CHECK(cudaGetLastError());
-    count_launches(3);
-  }
+  if (!support) support_device(intensity, d, ndim, support_threshold, support_out, scratch + 256, stream);
   unsigned long long host_flags[2];
-  QPB_CHECK(cudaMemcpyAsync(host_flags, flags.get(), sizeof(host_flags), cudaMemcpyDeviceToHost,
-                            stream));
+  QPB_CHECK(cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, stream));
   QPB_CHECK(cudaStreamSynchronize(stream));
   check_waits();
   if (host_flags[0]) throw InvalidArgument("intensity contains NaN or Inf");
@@ -182,42 +233,67 @@ void make_problem_device(const float* intensity, int ndim, const long long* shap
   }
 }
 
+void autocorrelation_support_host(const float* intensity, int ndim, const long long* shape,
+                                  float threshold, std::uint8_t* out) {
+  ProblemView v;
+  v.ndim = ndim;
+  if (ndim != 2 && ndim != 3) {
+    throw InvalidArgument("shape must be 2D or 3D, got ndim=" + std::to_string(ndim));
+  }
+  for (int a = 0; a < ndim; ++a) v.shape[a] = shape[a];
+  const Dims3 d = dims_of(v);
+  const auto n = static_cast<std::size_t>(d.n());
+  SetupArena& arena = setup_arena();
+  std::lock_guard<std::mutex> lock(arena.mutex);
+  const std::size_t in_bytes = align256(n * sizeof(float));
+  unsigned char* scratch = arena.reserve(in_bytes + align256(n) + support_scratch_bytes(d.n()));
+  auto* dev_in = reinterpret_cast<float*>(scratch);
+  std::uint8_t* dev_out = scratch + in_bytes;
+  const cudaStream_t s = *arena.stream;
+  QPB_CHECK(cudaMemcpyAsync(dev_in, intensity, n * sizeof(float), cudaMemcpyHostToDevice, s));
+  support_device(dev_in, d, ndim, threshold, dev_out, scratch + in_bytes + align256(n), s);
+  QPB_CHECK(cudaMemcpyAsync(out, dev_out, n, cudaMemcpyDeviceToHost, s));
+  QPB_CHECK(cudaStreamSynchronize(s));
+  check_waits();
+}
+
+std::size_t prepare_scratch_bytes(long long n) { return 256 + align256(static_cast<std::size_t>(n)); }
+
 double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
                               int lines, float* amp_fft, void* signed_out,
-                              std::uint8_t* support_fft, cudaStream_t stream) {
+                              std::uint8_t* support_fft, void* scratch, cudaStream_t stream) {
   const long long n = d.n();
-  DeviceBuffer<std::uint8_t> mask_fft(static_cast<std::size_t>(n));
-  DeviceBuffer<double> energy(1);
+  auto* energy = static_cast<double*>(scratch);
+  std::uint8_t* mask_fft = static_cast<std::uint8_t*>(scratch) + 256;
   roll<float>(q.amplitude, amp_fft, d, 1, true, stream);
   if (q.mask) {
-    roll<std::uint8_t>(q.mask, mask_fft.get(), d, 1, true, stream);
+    roll<std::uint8_t>(q.mask, mask_fft, d, 1, true, stream);
   } else {
-    QPB_CHECK(cudaMemsetAsync(mask_fft.get(), 0, static_cast<std::size_t>(n), stream));
+    QPB_CHECK(cudaMemsetAsync(mask_fft, 0, static_cast<std::size_t>(n), stream));
   }
   roll<std::uint8_t>(q.support, support_fft, d, 1, true, stream);
   nonzero_kernel<<<blocks_for(n), kThreads, 0, stream>>>(support_fft, n);
   QPB_CHECK(cudaGetLastError());
-  QPB_CHECK(cudaMemsetAsync(energy.get(), 0, sizeof(double), stream));
   switch (storage) {
     case AmpStorage::kF32:
       signed_kernel<float><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<float*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, static_cast<float*>(signed_out));
       break;
     case AmpStorage::kF16:
       signed_kernel<__half><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<__half*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, static_cast<__half*>(signed_out));
       break;
     case AmpStorage::kBF16:
       signed_kernel<__nv_bfloat16><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft.get(), n, L, S, lines, static_cast<__nv_bfloat16*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, static_cast<__nv_bfloat16*>(signed_out));
       break;
   }
   QPB_CHECK(cudaGetLastError());
-  energy_kernel<<<blocks_for(n), kThreads, 0, stream>>>(amp_fft, mask_fft.get(), n, energy.get());
+  energy_kernel<<<1, kEnergyThreads, 0, stream>>>(amp_fft, mask_fft, n, energy);
   QPB_CHECK(cudaGetLastError());
   count_launches(3);
   double host = 0.0;
-  QPB_CHECK(cudaMemcpyAsync(&host, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
+  QPB_CHECK(cudaMemcpyAsync(&host, energy, sizeof(double), cudaMemcpyDeviceToHost, stream));
   QPB_CHECK(cudaStreamSynchronize(stream));
   return host;
 }

@@ -486,25 +486,6 @@ int fast_pass_lines(const PassParams& p) {
   return fast_passes_enabled() && fast_pass_supports(p) ? fast_lines(p.L, p.S == 1) : 0;
 }
 
-std::vector<unsigned char> tile_amplitude(const std::vector<unsigned char>& amp,
-                                          std::size_t elem_size, long long n, int L, int S,
-                                          int lines) {
-  if (S == 1) return amp;  // rows: FFT order already has each CTA's lines contiguous
-  std::vector<unsigned char> out(amp.size());
-  const long long slab = static_cast<long long>(L) * S;
-  for (long long e = 0; e < n; ++e) {
-    const long long outer = e / slab;
-    const long long rem = e - outer * slab;
-    const long long j = rem / S;
-    const long long col = rem - j * S;
-    const long long tile = outer * (S / lines) + col / lines;
-    const long long c = col % lines;
-    const long long to = S > 1 ? (tile * L + j) * lines + c : (tile * lines + c) * L + j;
-    std::memcpy(&out[to * elem_size], &amp[e * elem_size], elem_size);
-  }
-  return out;
-}
-
 int take_fast_wait_failures() {
   int failures = 0;
   QPB_CHECK(cudaMemcpyFromSymbol(&failures, g_fast_wait_failures, sizeof(int)));

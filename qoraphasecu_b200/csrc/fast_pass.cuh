@@ -23,15 +23,6 @@ bool fast_passes_enabled();
 // Lines per CTA of the register-resident kernel for this pass (0: not used).
 int fast_pass_lines(const PassParams& p);
 
-// Reorders one per-problem array (n elements of elem_size bytes, FFT order)
-// into the CTA order of the register-resident pass along an axis of length L
-// and stride S with `lines` lines per CTA: each CTA's L x lines tile becomes
-// contiguous, element j of line c at (tile * L + j) * lines + c for columns
-// (S > 1) and (tile * lines + c) * L + j for rows.
-std::vector<unsigned char> tile_amplitude(const std::vector<unsigned char>& amp,
-                                          std::size_t elem_size, long long n, int L, int S,
-                                          int lines);
-
 // Number of CTAs whose bounded wait for their staged inputs gave up since the
 // last call (those CTAs wrote nothing); reading clears it. Synchronises.
 int take_fast_wait_failures();

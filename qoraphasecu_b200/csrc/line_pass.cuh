@@ -83,7 +83,8 @@ struct PassParams {
   int bump_counter;               // kUpd increments ctrl->counters[group]
   AmpStorage amp_storage;
   // The amplitude is stored in the CTA order of a register-resident modulus
-  // pass (tile_amplitude) instead of FFT order: one contiguous tile per CTA.
+  // pass (written so by the problem set-up's signed_kernel) instead of FFT
+  // order: one contiguous tile per CTA.
   int amp_tiled;
 };
 

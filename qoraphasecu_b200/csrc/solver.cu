@@ -346,10 +346,10 @@ void Solver::reset(const std::vector<ProblemView>& problems, std::uint64_t seed,
 
 // Problems into the solver's buffers: per problem the FFT-order amplitude,
 // mask and support, the signed amplitude in the storage type (in the modulus
-// pass's CTA order when that pass runs the register-resident kernel, so each
-// CTA stages its tile with one bulk copy) and the usable energy; then the
-// starts, drawn or given. The captured graphs stay valid: every buffer keeps
-// its address.
+// pass's CTA order when that pass tiles it, so each CTA stages its tile with
+// one bulk copy) and the usable energy, all prepared on the device (host
+// arrays are staged there first); then the starts, drawn or given. The
+// captured graphs stay valid: every buffer keeps its address.
 void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
                   const float2* start) {
   const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
@@ -360,40 +360,41 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   for (const ProblemView& q : problems) {
     if (q.on_device != on_device) throw InvalidArgument("problems mix host and device arrays");
   }
+  const auto n = static_cast<std::size_t>(n_);
+  auto round256 = [](std::size_t b) { return (b + 255) / 256 * 256; };
+  const std::size_t scratch = round256(prepare_scratch_bytes(n_));
+  const std::size_t amp_bytes = round256(n * sizeof(float));
+  const std::size_t staged = on_device ? 0 : amp_bytes + 2 * round256(n);
+  if (prep_.size() < scratch + staged) {
+    prep_ = DeviceBuffer<unsigned char>();
+    prep_ = DeviceBuffer<unsigned char>(scratch + staged);
+  }
   energies_.clear();
-  std::vector<float> amp_all;
-  std::vector<unsigned char> signed_all;
-  std::vector<std::vector<std::uint8_t>> supports;
-  if (on_device) {
-    // The same preparation on the device, from the caller's device arrays.
-    for (int q = 0; q < problems_; ++q) {
-      energies_.push_back(prepare_problem_device(
-          problems[q], d_, options_.amp_storage, mod.L, mod.S, lines,
-          amp_f_.get() + static_cast<std::size_t>(q) * n_,
-          amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
-          support_.get() + static_cast<std::size_t>(q) * spp_ * n_, stream_));
-    }
-  } else {
-    for (const ProblemView& q : problems) {
-      const auto amp = host_roll(q.amplitude, d_, true);
-      std::vector<std::uint8_t> mask(static_cast<std::size_t>(n_), 0);
-      if (q.mask) {
-        mask = host_roll(q.mask, d_, true);
-        for (auto& m : mask) m = m != 0;
+  for (int q = 0; q < problems_; ++q) {
+    ProblemView v = problems[q];
+    if (!on_device) {
+      // one problem at a time through the staging area (each preparation
+      // synchronises the stream before the next upload)
+      unsigned char* stage = prep_.get() + scratch;
+      auto* amp = reinterpret_cast<float*>(stage);
+      std::uint8_t* mask = stage + amp_bytes;
+      std::uint8_t* sup = mask + round256(n);
+      QPB_CHECK(cudaMemcpyAsync(amp, v.amplitude, n * sizeof(float), cudaMemcpyHostToDevice,
+                                stream_));
+      if (v.mask) {
+        QPB_CHECK(cudaMemcpyAsync(mask, v.mask, n, cudaMemcpyHostToDevice, stream_));
       }
-      auto sup = host_roll(q.support, d_, true);
-      for (auto& v : sup) v = v != 0;
-      energies_.push_back(usable_energy(amp, mask));
-      auto bytes = signed_amplitude(amp, mask, options_.amp_storage);
-      if (lines > 0) bytes = tile_amplitude(bytes, elem, n_, mod.L, mod.S, lines);
-      amp_all.insert(amp_all.end(), amp.begin(), amp.end());
-      signed_all.insert(signed_all.end(), bytes.begin(), bytes.end());
-      supports.push_back(std::move(sup));
+      QPB_CHECK(cudaMemcpyAsync(sup, v.support, n, cudaMemcpyHostToDevice, stream_));
+      v.amplitude = amp;
+      v.mask = v.mask ? mask : nullptr;
+      v.support = sup;
+      v.on_device = true;
     }
-    QPB_CHECK(cudaMemcpyAsync(amp_.get(), signed_all.data(), signed_all.size(),
-                              cudaMemcpyHostToDevice, stream_));
-    QPB_CHECK(cudaMemcpyAsync(amp_f_.get(), amp_all.data(), amp_all.size() * sizeof(float),
-                              cudaMemcpyHostToDevice, stream_));
+    energies_.push_back(prepare_problem_device(
+        v, d_, options_.amp_storage, mod.L, mod.S, lines,
+        amp_f_.get() + static_cast<std::size_t>(q) * n_,
+        amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
+        support_.get() + static_cast<std::size_t>(q) * spp_ * n_, prep_.get(), stream_));
   }
   QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
@@ -401,16 +402,12 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   set_ctrl(ctrl_.get(), ctrl, stream_);
   for (int q = 0; q < problems_; ++q) {
     std::uint8_t* first = support_.get() + static_cast<std::size_t>(q) * spp_ * n_;
-    if (!on_device) {
-      QPB_CHECK(cudaMemcpyAsync(first, supports[q].data(), supports[q].size(),
-                                cudaMemcpyHostToDevice, stream_));
-    }
     for (int s = 1; s < spp_; ++s) {
       QPB_CHECK(cudaMemcpyAsync(first + static_cast<std::size_t>(s) * n_, first,
                                 static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
     }
   }
-  stream_.sync();  // the host vectors above are released at the end of this scope
+  stream_.sync();
   errors_.assign(static_cast<std::size_t>(starts_), {});
   iteration_ = 0;
   run_iterations_ = 0;
@@ -821,10 +818,9 @@ void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
 }
 
 // ------------------------------------------------------------------- operators
-namespace {
-
-// Line plans (device twiddle tables) of the single operators, kept per device
-// for the process so that repeated calls allocate nothing for them.
+// Line plans (device twiddle tables) of the single operators and the problem
+// set-up, kept per device for the process so that repeated calls allocate
+// nothing for them.
 PlanCache& operator_plans() {
   static std::mutex mutex;
   static std::map<int, std::unique_ptr<PlanCache>> per_device;
@@ -835,6 +831,8 @@ PlanCache& operator_plans() {
   if (!slot) slot = std::make_unique<PlanCache>();
   return *slot;
 }
+
+namespace {
 
 struct OperatorContext {
   Dims3 d;
@@ -938,36 +936,6 @@ void gaussian_blur(const float* image, int ndim, const long long* shape, float s
   ctx.stream.sync();
   check_waits();
   for (long long i = 0; i < n; ++i) out[i] = host[i].x;
-}
-
-void autocorrelation_support(const float* intensity, int ndim, const long long* shape,
-                             float threshold, std::uint8_t* out) {
-  const Dims3 d = dims_of(view_of(ndim, shape));
-  const long long n = d.n();
-  OperatorContext ctx(d, ndim);
-  const auto ordered = host_roll(intensity, d, true);
-  std::vector<float2> host(static_cast<std::size_t>(n));
-  for (long long i = 0; i < n; ++i) host[i] = {ordered[i], 0.0f};
-  auto w = upload(host, ctx.stream);
-  for (int axis3 = ctx.runner.outer(); axis3 < 3; ++axis3) {
-    PassParams p = ctx.runner.params(Mode::kInv, axis3, 1);
-    p.w = w.get();
-    ctx.runner.launch(Mode::kInv, axis3, p, ctx.stream);
-  }
-  QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
-                            cudaMemcpyDeviceToHost, ctx.stream));
-  ctx.stream.sync();
-  check_waits();
-  // Unitary scale, |.|, centre-origin, threshold against the maximum.
-  const float s = 1.0f / std::sqrt(static_cast<float>(n));
-  std::vector<float> ac(static_cast<std::size_t>(n));
-  for (long long i = 0; i < n; ++i) {
-    const float re = host[i].x * s, im = host[i].y * s;
-    ac[i] = std::sqrt(re * re + im * im);
-  }
-  const auto centred = host_roll(ac.data(), d, false);
-  const float level = threshold * *std::max_element(centred.begin(), centred.end());
-  for (long long i = 0; i < n; ++i) out[i] = centred[i] > level;
 }
 
 void half_support(const std::uint8_t* support, int ndim, const long long* shape, int axis,

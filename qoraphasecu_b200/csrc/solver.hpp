@@ -182,6 +182,10 @@ class PassRunner {
   const LinePlan* plans_[3];
 };
 
+// Line plans shared by the single operators and the problem set-up, one cache
+// per device for the process.
+PlanCache& operator_plans();
+
 // DeviceSelect makes `requested` (>= 0) the calling thread's device before any
 // allocation and remembers the device in use.
 struct DeviceSelect {
@@ -286,6 +290,7 @@ class Solver {
   long long amp_stride_ = 0;         // elements between problems' amplitudes in amp_
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
   DeviceBuffer<float> amp_f_;        // FP32 FFT-order amplitude, for the random starts
+  DeviceBuffer<unsigned char> prep_;  // problem set-up: scratch, and host arrays staged
   bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
   bool resident_ = false;            // iterations run by the resident kernel
   DeviceBuffer<float2> x_;
@@ -317,9 +322,6 @@ class Solver {
 float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storage);
 void support_project_host(const std::uint8_t* support, float2* obj, long long count);
 void gaussian_blur(const float* image, int ndim, const long long* shape, float sigma, float* out);
-// Loose support: |IFFT(intensity)| > threshold * max, centre-origin (problem.cpp:72-88).
-void autocorrelation_support(const float* intensity, int ndim, const long long* shape,
-                             float threshold, std::uint8_t* out);
 // aligned_error (metrics.cpp:17-86) of `batch` candidates a[b] (numel complex64
 // each) against one reference, on the device; out[b] = the smaller of the
 // direct and twin errors. Host arrays.
