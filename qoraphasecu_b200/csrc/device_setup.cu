@@ -257,14 +257,13 @@ void autocorrelation_support_host(const float* intensity, int ndim, const long l
   check_waits();
 }
 
-std::size_t prepare_scratch_bytes(long long n) { return 256 + align256(static_cast<std::size_t>(n)); }
+std::size_t prepare_scratch_bytes(long long n) { return align256(static_cast<std::size_t>(n)); }
 
-double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
-                              int lines, float* amp_fft, void* signed_out,
-                              std::uint8_t* support_fft, void* scratch, cudaStream_t stream) {
+void prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
+                            int lines, float* amp_fft, void* signed_out, std::uint8_t* support_fft,
+                            void* scratch, double* energy, cudaStream_t stream) {
   const long long n = d.n();
-  auto* energy = static_cast<double*>(scratch);
-  std::uint8_t* mask_fft = static_cast<std::uint8_t*>(scratch) + 256;
+  std::uint8_t* mask_fft = static_cast<std::uint8_t*>(scratch);
   roll<float>(q.amplitude, amp_fft, d, 1, true, stream);
   if (q.mask) {
     roll<std::uint8_t>(q.mask, mask_fft, d, 1, true, stream);
@@ -292,10 +291,6 @@ double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage,
   energy_kernel<<<1, kEnergyThreads, 0, stream>>>(amp_fft, mask_fft, n, energy);
   QPB_CHECK(cudaGetLastError());
   count_launches(3);
-  double host = 0.0;
-  QPB_CHECK(cudaMemcpyAsync(&host, energy, sizeof(double), cudaMemcpyDeviceToHost, stream));
-  QPB_CHECK(cudaStreamSynchronize(stream));
-  return host;
 }
 
 }  // namespace qpb

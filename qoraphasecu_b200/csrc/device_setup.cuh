@@ -31,17 +31,19 @@ void make_problem_device(const float* intensity, int ndim, const long long* shap
 void autocorrelation_support_host(const float* intensity, int ndim, const long long* shape,
                                   float threshold, std::uint8_t* out);
 
-// Device bytes of `scratch` that prepare_problem_device needs for n elements.
+// Device bytes of `scratch` that prepare_problem_device needs for n elements
+// (a multiple of 256).
 std::size_t prepare_scratch_bytes(long long n);
 
 // One problem's solver inputs from its device arrays (centre-origin): the FFT-
 // order FP32 amplitude, the signed amplitude (-1 masked) in `storage` written
 // to `signed_out` in the modulus pass's CTA order when `lines` > 0 and S > 1,
-// and the FFT-order 0/1 support. Returns the usable energy (sum of A^2 over
-// unmasked pixels, in one fixed order: the same bits on every call);
-// synchronises `stream`. `scratch`: prepare_scratch_bytes(n) device bytes.
-double prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
-                              int lines, float* amp_fft, void* signed_out,
-                              std::uint8_t* support_fft, void* scratch, cudaStream_t stream);
+// the FFT-order 0/1 support, and the usable energy (sum of A^2 over unmasked
+// pixels, in one fixed order: the same bits on every call) into the device
+// double `energy`. Enqueued on `stream`, which it does not synchronise.
+// `scratch`: prepare_scratch_bytes(n) device bytes, in use until the work ends.
+void prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
+                            int lines, float* amp_fft, void* signed_out, std::uint8_t* support_fft,
+                            void* scratch, double* energy, cudaStream_t stream);
 
 }  // namespace qpb

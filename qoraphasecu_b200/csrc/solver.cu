@@ -360,22 +360,26 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   for (const ProblemView& q : problems) {
     if (q.on_device != on_device) throw InvalidArgument("problems mix host and device arrays");
   }
+  // prep_: the problems' energies, then per problem its set-up scratch and,
+  // for host arrays, the staged amplitude, mask and support
   const auto n = static_cast<std::size_t>(n_);
   auto round256 = [](std::size_t b) { return (b + 255) / 256 * 256; };
-  const std::size_t scratch = round256(prepare_scratch_bytes(n_));
+  const std::size_t head = round256(static_cast<std::size_t>(problems_) * sizeof(double));
+  const std::size_t scratch = prepare_scratch_bytes(n_);
   const std::size_t amp_bytes = round256(n * sizeof(float));
   const std::size_t staged = on_device ? 0 : amp_bytes + 2 * round256(n);
-  if (prep_.size() < scratch + staged) {
+  const std::size_t per_problem = scratch + staged;
+  const std::size_t bytes = head + static_cast<std::size_t>(problems_) * per_problem;
+  if (prep_.size() < bytes) {
     prep_ = DeviceBuffer<unsigned char>();
-    prep_ = DeviceBuffer<unsigned char>(scratch + staged);
+    prep_ = DeviceBuffer<unsigned char>(bytes);
   }
-  energies_.clear();
+  auto* energies = reinterpret_cast<double*>(prep_.get());
   for (int q = 0; q < problems_; ++q) {
     ProblemView v = problems[q];
+    unsigned char* region = prep_.get() + head + static_cast<std::size_t>(q) * per_problem;
     if (!on_device) {
-      // one problem at a time through the staging area (each preparation
-      // synchronises the stream before the next upload)
-      unsigned char* stage = prep_.get() + scratch;
+      unsigned char* stage = region + scratch;
       auto* amp = reinterpret_cast<float*>(stage);
       std::uint8_t* mask = stage + amp_bytes;
       std::uint8_t* sup = mask + round256(n);
@@ -390,12 +394,15 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
       v.support = sup;
       v.on_device = true;
     }
-    energies_.push_back(prepare_problem_device(
-        v, d_, options_.amp_storage, mod.L, mod.S, lines,
-        amp_f_.get() + static_cast<std::size_t>(q) * n_,
-        amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
-        support_.get() + static_cast<std::size_t>(q) * spp_ * n_, prep_.get(), stream_));
+    prepare_problem_device(v, d_, options_.amp_storage, mod.L, mod.S, lines,
+                           amp_f_.get() + static_cast<std::size_t>(q) * n_,
+                           amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
+                           support_.get() + static_cast<std::size_t>(q) * spp_ * n_, region,
+                           energies + q, stream_);
   }
+  energies_.assign(static_cast<std::size_t>(problems_), 0.0);
+  QPB_CHECK(cudaMemcpyAsync(energies_.data(), energies, energies_.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream_));
   QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
   const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
