@@ -301,6 +301,9 @@ def workload_uneven(args):
     result = {}
 
     def run():
+        # the previous call's results are dropped first, as a caller that
+        # consumed them would, so their host memory can be reused
+        result.clear()
         with qpc.BatchSolver(problems, starts=4, seed=0, sync_every=50) as solver:
             solver.run(recipe)
             result["runs"] = solver.results()

@@ -171,23 +171,18 @@ void BatchSolver::results(float2* objects, std::uint8_t* supports, float* errors
   std::vector<long long> off(where_.size(), 0);
   for (std::size_t q = 1; q < where_.size(); ++q) off[q] = off[q - 1] + spp_ * numel_[q - 1];
   for (Class& c : classes_) {
-    const long long n = c.solver->numel();
-    const std::size_t cells = static_cast<std::size_t>(c.solver->starts()) * n;
-    std::vector<float2> o(objects ? cells : 0);
-    std::vector<std::uint8_t> s(supports ? cells : 0);
-    std::vector<float> e(errors ? static_cast<std::size_t>(c.solver->starts()) * errs : 0);
-    c.solver->results(objects ? o.data() : nullptr, supports ? s.data() : nullptr,
-                      errors ? e.data() : nullptr);
+    // each member problem's block goes straight to its place in the output
+    std::vector<float2*> o(c.members.size(), nullptr);
+    std::vector<std::uint8_t*> s(c.members.size(), nullptr);
+    std::vector<float*> e(c.members.size(), nullptr);
     for (std::size_t j = 0; j < c.members.size(); ++j) {
       const int q = c.members[j];
-      const std::size_t block = static_cast<std::size_t>(spp_) * n;
-      if (objects) std::copy_n(o.begin() + j * block, block, objects + off[q]);
-      if (supports) std::copy_n(s.begin() + j * block, block, supports + off[q]);
-      if (errors) {
-        const std::size_t eb = static_cast<std::size_t>(spp_) * errs;
-        std::copy_n(e.begin() + j * eb, eb, errors + static_cast<std::size_t>(q) * eb);
-      }
+      if (objects) o[j] = objects + off[q];
+      if (supports) s[j] = supports + off[q];
+      if (errors) e[j] = errors + static_cast<std::size_t>(q) * spp_ * errs;
     }
+    c.solver->results_per_problem(objects ? o.data() : nullptr, supports ? s.data() : nullptr,
+                                  errors ? e.data() : nullptr);
   }
 }
 

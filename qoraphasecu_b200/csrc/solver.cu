@@ -804,22 +804,50 @@ void Solver::results_device(float2* objects, std::uint8_t* supports, float* erro
 }
 
 void Solver::results(float2* objects, std::uint8_t* supports, float* errors) {
-  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  const std::size_t block = static_cast<std::size_t>(spp_) * n_;
+  const std::size_t count = error_count();
+  std::vector<float2*> o(static_cast<std::size_t>(problems_), nullptr);
+  std::vector<std::uint8_t*> s(o.size(), nullptr);
+  std::vector<float*> e(o.size(), nullptr);
+  for (std::size_t q = 0; q < o.size(); ++q) {
+    if (objects) o[q] = objects + q * block;
+    if (supports) s[q] = supports + q * block;
+    if (errors) e[q] = errors + q * spp_ * count;
+  }
+  results_per_problem(o.data(), s.data(), e.data());
+}
+
+void Solver::results_per_problem(float2* const* objects, std::uint8_t* const* supports,
+                                 float* const* errors) {
+  // centre-origin copies on the device, then one transfer per problem
+  // straight into the caller's memory
+  const std::size_t block = static_cast<std::size_t>(spp_) * n_;
   if (objects) {
     roll<float2>(x_.get(), w_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(objects, w_.get(), total * sizeof(float2), cudaMemcpyDeviceToHost,
-                              stream_));
     wave_valid_ = false;
+    for (int q = 0; q < problems_; ++q) {
+      if (!objects[q]) continue;
+      QPB_CHECK(cudaMemcpyAsync(objects[q], w_.get() + q * block, block * sizeof(float2),
+                                cudaMemcpyDeviceToHost, stream_));
+    }
   }
   if (supports) {
     roll<std::uint8_t>(support_.get(), saved_.get(), d_, starts_, false, stream_);
-    QPB_CHECK(cudaMemcpyAsync(supports, saved_.get(), total, cudaMemcpyDeviceToHost, stream_));
+    for (int q = 0; q < problems_; ++q) {
+      if (!supports[q]) continue;
+      QPB_CHECK(cudaMemcpyAsync(supports[q], saved_.get() + q * block, block,
+                                cudaMemcpyDeviceToHost, stream_));
+    }
   }
   stream_.sync();
   if (errors) {
     const std::size_t count = error_count();
-    for (int s = 0; s < starts_; ++s) {
-      std::copy(errors_[s].begin(), errors_[s].end(), errors + static_cast<std::size_t>(s) * count);
+    for (int q = 0; q < problems_; ++q) {
+      if (!errors[q]) continue;
+      for (int j = 0; j < spp_; ++j) {
+        const auto& row = errors_[static_cast<std::size_t>(q) * spp_ + j];
+        std::copy(row.begin(), row.end(), errors[q] + static_cast<std::size_t>(j) * count);
+      }
     }
   }
 }

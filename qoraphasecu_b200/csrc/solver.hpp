@@ -224,6 +224,11 @@ class Solver {
   cudaStream_t stream() const { return stream_; }
   // objects: starts * numel complex64; supports: starts * numel; errors: starts * error_count().
   void results(float2* objects, std::uint8_t* supports, float* errors);
+  // As results(), each problem's block of starts to its own host place:
+  // objects[q] (starts-per-problem * numel complex64), supports[q], errors[q]
+  // (starts-per-problem * error_count()); a null array, or a null entry, skips.
+  void results_per_problem(float2* const* objects, std::uint8_t* const* supports,
+                           float* const* errors);
   // As results(), objects and supports written to device memory (centre-origin)
   // on the solver's stream, which is synchronised before returning; errors on the host.
   void results_device(float2* objects, std::uint8_t* supports, float* errors);
