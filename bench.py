@@ -295,20 +295,31 @@ def workload_uneven(args):
 
     batch = workloads.uneven_batch(count=64, seed=2000)
     recipe = workloads.uneven_recipe()
-    problems = [qpc.make_problem(b[1], mask=b[2]) for b in batch]
+    intensities = [b[1] for b in batch]
+    masks = [b[2] for b in batch]
     sides = [int(b[1].shape[0]) for b in batch]
     elements = sum(s * s for s in sides)
     result = {}
 
+    # Each call: make_problem for every intensity (autocorrelation supports),
+    # the recipe, the results; the previous call's results are dropped first,
+    # as a caller that consumed them would, so their host memory is reused.
     def run():
-        # the previous call's results are dropped first, as a caller that
-        # consumed them would, so their host memory can be reused
+        result.clear()
+        result["runs"] = qpc.reconstruct_batch(intensities, masks=masks, recipe=recipe, starts=4,
+                                               seed=0, sync_every=50)
+
+    s = _timed(run, warmup=args.warmup, reps=args.steps)
+    qpc.api.clear_cache()
+    problems = [qpc.make_problem(i, mask=m) for i, m in zip(intensities, masks)]
+
+    def run_new_solver():
         result.clear()
         with qpc.BatchSolver(problems, starts=4, seed=0, sync_every=50) as solver:
             solver.run(recipe)
-            result["runs"] = solver.results()
+            result["runs"] = [tuple(r) for r in solver.results()]
 
-    s = _timed(run, warmup=args.warmup, reps=args.steps)
+    s_new = _timed(run_new_solver, warmup=1, reps=args.steps)
     iters = recipe.iterations()
     best = [min(r.error for r in runs) for runs in result["runs"]]
     per_side = {}
@@ -316,11 +327,14 @@ def workload_uneven(args):
         per_side.setdefault(side, []).append(b)
     return {
         "workload": "uneven batch: 64 problems, sides {64,128,256,512}, 4 starts, "
-                    "repeat(4, HIO(50), Shrinkwrap(rms 0.3)), ER(100); each timed call builds "
-                    "one BatchSolver (uploads, random starts) and runs the recipe; the "
-                    "warm-up calls leave the autotuner's choices cached",
+                    "repeat(4, HIO(50), Shrinkwrap(rms 0.3)), ER(100); each timed call is one "
+                    "reconstruct_batch over the 64 host intensities (make_problem with "
+                    "autocorrelation supports, the batch solver of the previous call reloaded, "
+                    "random starts, the recipe, host results); the warm-up calls leave the "
+                    "autotuner's choices and the solver cached",
         "problems_per_side": {str(k): len(v) for k, v in sorted(per_side.items())},
         "seconds": s,
+        "seconds_new_batch_solver": s_new,
         "start_iterations_per_s": 64 * 4 * iters / s,
         "element_iterations_per_s": 4 * elements * iters / s,
         "best_error_median_per_side": {str(k): float(np.median(v))

@@ -183,11 +183,13 @@ QPB_API qpb_status qpb_create_batch(const qpb_problem* problems, size_t n_proble
 QPB_API qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);
 
 /* Loads new problems into an existing solver (no counterpart in the reference):
- * the same number of problems of the solver's shape, host or device arrays as
- * at creation; starts drawn from `seed`, or given in `start` (NULL = drawn).
- * Device buffers, the schedule and the captured CUDA graphs are kept, so a
- * caller reconstructing a stream of same-shape patterns pays for allocation
- * and graph capture once. Error histories start afresh. */
+ * the same number of problems as at creation, problem q in the shape problem q
+ * had then (a batch of several shapes included), host or device arrays as at
+ * creation; starts drawn from `seed` as a new solver would draw them, or given
+ * in `start` (NULL = drawn; given device starts need one shape). Device
+ * buffers, the schedule and the captured CUDA graphs are kept, so a caller
+ * reconstructing a stream of same-shape patterns pays for allocation and graph
+ * capture once. Error histories start afresh. */
 QPB_API qpb_status qpb_reset(qpb_solver* solver, const qpb_problem* problems, size_t n_problems,
                              uint64_t seed, const float* start);
 

@@ -540,6 +540,31 @@ class BatchSolver:
         if progress is not None:
             self.set_progress(progress)
 
+    def reset(self, problems, *, seed: int | None = None, init=None):
+        """Loads new problems, problem q in the shape problem q had at
+        construction (host or device arrays as then), and draws new starts (or
+        takes ``init``, one start array per problem), keeping the device
+        buffers, schedules and captured graphs. Error histories start afresh."""
+        problems = list(problems)
+        if len(problems) != len(self.problems):
+            raise ValueError(f"reset needs {len(self.problems)} problems, got {len(problems)}")
+        for q, (new, old) in enumerate(zip(problems, self.problems)):
+            if tuple(new.shape) != tuple(old.shape):
+                raise ValueError(f"problem {q} has shape {tuple(new.shape)}, the batch was built "
+                                 f"with {tuple(old.shape)}")
+        start = None
+        if init is not None:
+            if len(init) != len(problems):
+                raise ValueError(f"init has {len(init)} entries for {len(problems)} problems")
+            start = np.concatenate([_start(i, p.shape, self._starts).ravel()
+                                    for i, p in zip(init, problems)])
+        views = (_lib.Problem * len(problems))(*[p._c() for p in problems])
+        ptr = None if start is None else ctypes.c_void_p(start.ctypes.data)
+        _lib.check(self._lib.qpb_reset(self._handle, views, len(problems),
+                                       0 if seed is None else seed, ptr))
+        self.problems = problems
+        self._views = views
+
     def set_progress(self, fn):
         """``fn(iteration, errors)`` every ``sync_every`` iterations; ``errors``
         holds problems * starts values, problem by problem."""
@@ -609,7 +634,9 @@ def reconstruct_batch(intensities, *, supports=None, masks=None, recipe=None, st
     """``reconstruct`` over many intensities of any mix of shapes in one batch
     (:class:`BatchSolver`); returns one Reconstruction (starts == 1) or
     Ensemble per intensity, in order. ``supports`` / ``masks``: None or one
-    entry (possibly None) per intensity."""
+    entry (possibly None) per intensity. The batch solver is kept for the next
+    call with the same shapes in the same order and options (one per thread;
+    clear_cache() releases it)."""
     intensities = list(intensities)
     supports = [None] * len(intensities) if supports is None else list(supports)
     masks = [None] * len(intensities) if masks is None else list(masks)
@@ -617,9 +644,35 @@ def reconstruct_batch(intensities, *, supports=None, masks=None, recipe=None, st
         raise ValueError("supports and masks need one entry per intensity")
     problems = [make_problem(i, s, m, support_threshold)
                 for i, s, m in zip(intensities, supports, masks)]
-    with BatchSolver(problems, starts=starts, **options) as solver:
+    seed = options.pop("seed", None)
+    init = options.pop("init", None)
+    progress = options.pop("progress", None)
+    # like reconstruct(): the batch solver of the last call with the same
+    # shapes and options is reloaded (BatchSolver.reset) instead of rebuilt
+    try:
+        key = ("batch", tuple(tuple(p.shape) for p in problems), problems[0].on_device, starts,
+               tuple(sorted(options.items())), _current_device())
+        hash(key)
+    except TypeError:
+        key = None
+    solver = _cached_solvers().get(key) if key is not None else None
+    if solver is not None and solver._handle:
+        solver.reset(problems, seed=seed, init=init)
+    else:
+        solver = BatchSolver(problems, starts=starts, seed=seed, init=init, **options)
+        if key is not None:
+            cache = _cached_solvers()
+            for old in [k for k in cache if k[0] == "batch"]:
+                cache.pop(old).close()
+            cache[key] = solver
+    try:
+        solver.set_progress(progress)
         solver.run(default_recipe() if recipe is None else recipe)
         runs = solver.results()
+        solver.set_progress(None)
+    finally:
+        if key is None:
+            solver.close()
     return [r[0] if starts == 1 else Ensemble(tuple(r)) for r in runs]
 
 
@@ -719,8 +772,8 @@ def _cached_solvers() -> dict:
 
 
 def clear_cache() -> None:
-    """Releases the solvers (and their device memory) that reconstruct() keeps
-    for reuse on this thread."""
+    """Releases the solvers (and their device memory) that reconstruct() and
+    reconstruct_batch() keep for reuse on this thread."""
     for solver in _cached_solvers().values():
         solver.close()
     _cached_solvers().clear()

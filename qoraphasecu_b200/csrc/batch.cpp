@@ -6,6 +6,7 @@
 #include <array>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 
 namespace qpb {
 
@@ -188,9 +189,37 @@ void BatchSolver::results(float2* objects, std::uint8_t* supports, float* errors
 
 void BatchSolver::reset(std::vector<ProblemView> problems, std::uint64_t seed,
                         const float2* start) {
-  if (classes_.size() != 1) throw InvalidArgument("reset needs problems of one shape");
-  for (ProblemView& q : problems) q.on_device = on_device_;
-  classes_[0].solver->reset(problems, seed, start);
+  if (problems.size() != where_.size()) {
+    throw InvalidArgument("reset needs as many problems as the batch was built with");
+  }
+  for (std::size_t q = 0; q < problems.size(); ++q) {
+    problems[q].on_device = on_device_;
+    if (dims_of(problems[q]).n() != numel_[q]) {
+      throw InvalidArgument("reset needs problem " + std::to_string(q) + " in its original shape");
+    }
+  }
+  if (classes_.size() == 1) {
+    classes_[0].solver->reset(problems, seed, start);
+    iteration_ = 0;
+    return;
+  }
+  if (start && on_device_) throw InvalidArgument("given starts on the device need problems of one shape");
+  std::vector<long long> start_off(problems.size(), 0);
+  for (std::size_t q = 1; q < problems.size(); ++q) {
+    start_off[q] = start_off[q - 1] + static_cast<long long>(spp_) * numel_[q - 1];
+  }
+  for (Class& c : classes_) {
+    std::vector<ProblemView> views;
+    std::vector<float2> given;
+    for (int q : c.members) {
+      views.push_back(problems[q]);
+      if (start) {
+        const float2* src = start + start_off[q];
+        given.insert(given.end(), src, src + static_cast<std::size_t>(spp_) * numel_[q]);
+      }
+    }
+    c.solver->reset(views, seed, start ? given.data() : nullptr);
+  }
   iteration_ = 0;
 }
 

@@ -28,8 +28,9 @@ class BatchSolver {
   BatchSolver& operator=(const BatchSolver&) = delete;
 
   void run(const OpDesc* ops, std::size_t count);
-  // Solver::reset for a batch of one shape class: new problems (same count and
-  // shape, host or device arrays as at construction), new starts.
+  // Solver::reset for every shape class: new problems (the same count, problem
+  // q of problem q's shape at construction, host or device arrays as then),
+  // new starts drawn from `seed` as a new batch would draw them, or given.
   void reset(std::vector<ProblemView> problems, std::uint64_t seed, const float2* start);
   bool on_device() const { return on_device_; }
   std::size_t error_count() const { return classes_[0].solver->error_count(); }

@@ -51,6 +51,65 @@ def test_batch_equals_problems_run_alone(gpu):
             np.testing.assert_allclose(r.errors, a.errors, rtol=1e-6)
 
 
+def test_batch_reset_equals_a_new_batch(gpu):
+    """BatchSolver.reset with new problems of the same shapes (several shape
+    classes) gives what a new batch built on them gives, bit for bit."""
+    first = [qpc.make_problem(i, support=s, mask=m) for i, s, m in problems_of(SHAPES)]
+    second = [qpc.make_problem(i, support=s, mask=m)
+              for i, s, m in problems_of([(shape, m + 2) for shape, m in SHAPES])]
+    recipe = Recipe(HIO(8), Shrinkwrap(method="rms"), ER(6))
+    with qpc.BatchSolver(first, starts=2, seed=5, sync_every=4, schedule="streamed") as b:
+        b.run(recipe)
+        b.reset(second, seed=9)
+        b.run(recipe)
+        reused = b.results()
+    with qpc.BatchSolver(second, starts=2, seed=9, sync_every=4, schedule="streamed") as b:
+        b.run(recipe)
+        fresh = b.results()
+    for runs_a, runs_b in zip(reused, fresh, strict=True):
+        for a, r in zip(runs_a, runs_b, strict=True):
+            assert len(a.errors) == recipe.iterations()
+            np.testing.assert_array_equal(a.object, r.object)
+            np.testing.assert_array_equal(a.support, r.support)
+            np.testing.assert_allclose(a.errors, r.errors, rtol=1e-6)
+    with qpc.BatchSolver(first, starts=2, seed=5) as b:
+        with pytest.raises(ValueError):
+            b.reset(second[:-1])
+        with pytest.raises(ValueError):
+            b.reset(second[::-1])
+
+
+def test_reconstruct_batch_reuses_its_solver(gpu):
+    qpc.api.clear_cache()
+    data1 = problems_of(SHAPES[:4])
+    data2 = problems_of([(shape, m + 2) for shape, m in SHAPES[:4]])
+    recipe = Recipe(HIO(6), ER(4))
+
+    def call(data):
+        return qpc.reconstruct_batch([d[0] for d in data], supports=[d[1] for d in data],
+                                     masks=[d[2] for d in data], recipe=recipe, starts=2, seed=3,
+                                     sync_every=5)
+
+    def batch_solvers():
+        return [v for k, v in qpc.api._cached_solvers().items() if k[0] == "batch"]
+
+    call(data1)
+    kept = batch_solvers()
+    assert len(kept) == 1
+    second = call(data2)
+    assert batch_solvers() == kept
+    problems = [qpc.make_problem(i, support=s, mask=m) for i, s, m in data2]
+    with qpc.BatchSolver(problems, starts=2, seed=3, sync_every=5) as b:
+        b.run(recipe)
+        fresh = b.results()
+    for ens, runs in zip(second, fresh, strict=True):
+        for x, y in zip(ens, runs, strict=True):
+            np.testing.assert_array_equal(x.object, y.object)
+            np.testing.assert_array_equal(x.support, y.support)
+    qpc.api.clear_cache()
+    assert batch_solvers() == []
+
+
 def test_batch_matches_fp64(gpu):
     data = problems_of(SHAPES[:4])
     recipe = Recipe(HIO(10), Shrinkwrap(), ER(10))
