@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   }
   float2* __restrict__ wl = p.w + base;
   float2* __restrict__ xl = p.x + base;
-  const float2* __restrict__ tw = p.twiddle;
+  const float2* __restrict__ tw = p.stage_twiddle;
   // A row's T threads share a warp, so its exchanges need warp barriers only.
   constexpr bool kWarpLocal = ROWS && T <= 32;
 
@@ -411,6 +411,23 @@ template <int L>
 int lines_per_cta(bool rows) {
   return rows ? Tiling<L, true>::LINES : Tiling<L, false>::LINES;
 }
+
+}  // namespace
+
+StageGeometry stage_geometry(int L) {
+  switch (L) {
+    case 16: return stage_geometry_of<16>();
+    case 32: return stage_geometry_of<32>();
+    case 64: return stage_geometry_of<64>();
+    case 128: return stage_geometry_of<128>();
+    case 256: return stage_geometry_of<256>();
+    case 512: return stage_geometry_of<512>();
+    case 1024: return stage_geometry_of<1024>();
+    default: return {};
+  }
+}
+
+namespace {
 
 int fast_lines(int L, bool rows) {
   switch (L) {

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "stage_table.hpp"
 
 namespace qpb {
 
@@ -62,11 +63,16 @@ const LinePlan& PlanCache::get(int length) {
     const double angle = -2.0 * M_PI * static_cast<double>(k) / static_cast<double>(length);
     host[k] = {static_cast<float>(std::cos(angle)), static_cast<float>(std::sin(angle))};
   }
+  // The stage-major table holds entries of the same W_L^e, so both tables
+  // carry identical values.
+  const StageGeometry g = stage_geometry(length);
+  for (int i = 0; i < g.count; ++i) host.push_back(host[stage_twiddle_exponent(g, length, i)]);
   void* dev = nullptr;
   QPB_CHECK(cudaMalloc(&dev, host.size() * sizeof(float2)));
   allocations_.push_back(dev);
   QPB_CHECK(cudaMemcpy(dev, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice));
   plan.twiddle = static_cast<const float2*>(dev);
+  plan.stage_twiddle = g.count > 0 ? plan.twiddle + length : plan.twiddle;
   return plans_.emplace(length, plan).first->second;
 }
 

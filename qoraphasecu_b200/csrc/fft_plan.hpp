@@ -24,6 +24,9 @@ struct LinePlan {
   int stages = 0;
   int radix[kMaxStages] = {};
   const float2* twiddle = nullptr;  // device, `length` entries
+  // device, the stage-major table of the register-resident transform
+  // (stage_table.hpp) for lengths that have one, else `twiddle`
+  const float2* stage_twiddle = nullptr;
 };
 
 // Radix sequence for a line of length `n` (throws InvalidArgument when a prime

@@ -17,6 +17,7 @@
 
 #include "butterfly.cuh"
 #include "common.cuh"
+#include "stage_table.hpp"
 
 namespace qpb {
 
@@ -32,6 +33,9 @@ struct Geometry {
   static constexpr int R2 = L / (R0 * R1);
   static constexpr int STAGES = L <= 16 ? 1 : (R2 == 1 ? 2 : 3);
   static constexpr int PITCH = swz(L) + 1;
+  // Offsets of stages 1 and 2 in the stage-major twiddle table.
+  static constexpr int OFF1 = 0;
+  static constexpr int OFF2 = (R1 - 1) * R0;
   static_assert(R0 * R1 * R2 == L, "bad factorisation");
   static_assert(R2 <= E && R1 <= E, "radix above the register count");
 };
@@ -65,14 +69,18 @@ __device__ __forceinline__ void line_sync() {
 // others exchange through the line's shared-memory row. TRAIL orders the
 // exchange's reads before any later write of the row; a caller may drop it
 // when a block barrier separates them anyway.
-template <int L, int R, int NS, bool LAST, bool INV, bool WARP_LOCAL = false, bool TRAIL = true>
+//
+// `tw` is the stage-major twiddle table (stage_twiddle_exponent): this
+// stage's W_L^{r k L/(NS R)} sits at tw[OFF + (r - 1) NS + k], so the
+// threads of a line, whose k are consecutive, read consecutive entries.
+template <int L, int R, int NS, int OFF, bool LAST, bool INV, bool WARP_LOCAL = false,
+          bool TRAIL = true>
 __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
                                       const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
   constexpr int E = G::E;
   constexpr int T = G::T;
   constexpr int Q = E / R;
-  constexpr int STEP = L / (NS * R);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     float2 u[R];
@@ -83,7 +91,7 @@ __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
     if constexpr (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const float2 w = __ldg(tw + r * k * STEP);
+        const float2 w = __ldg(tw + OFF + (r - 1) * NS + k);
         u[r] = INV ? cmulc(u[r], w) : cmul(u[r], w);
       }
     }
@@ -118,15 +126,28 @@ __device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
   using G = Geometry<L>;
   static_assert(!WARP_LOCAL || G::T <= 32, "a line spans several warps");
   if constexpr (G::STAGES == 1) {
-    stage<L, G::R0, 1, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else if constexpr (G::STAGES == 2) {
-    stage<L, G::R0, 1, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
-    stage<L, G::R1, G::R0, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
+    stage<L, G::R1, G::R0, G::OFF1, true, INV, WARP_LOCAL>(v, t, tw, row);
   } else {
-    stage<L, G::R0, 1, false, INV, WARP_LOCAL>(v, t, tw, row);
-    stage<L, G::R1, G::R0, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
-    stage<L, G::R2, G::R0 * G::R1, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R1, G::R0, G::OFF1, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
+    stage<L, G::R2, G::R0 * G::R1, G::OFF2, true, INV, WARP_LOCAL>(v, t, tw, row);
   }
+}
+
+template <int L>
+constexpr StageGeometry stage_geometry_of() {
+  using G = Geometry<L>;
+  StageGeometry g;
+  g.stages = G::STAGES;
+  g.radix[0] = G::R0;
+  g.radix[1] = G::R1;
+  g.radix[2] = G::R2;
+  g.count = (G::STAGES >= 2 ? (G::R1 - 1) * G::R0 : 0) +
+            (G::STAGES >= 3 ? (G::R2 - 1) * G::R0 * G::R1 : 0);
+  return g;
 }
 
 }  // namespace qpb

@@ -63,6 +63,7 @@ struct PassParams {
   Ctrl* ctrl;
   LevelAcc* level;                // [batch], kBlur with level != 0
   const float2* twiddle;          // W_L^k, k < L
+  const float2* stage_twiddle;    // the register-resident passes' stage-major table
   long long n;                    // elements per start
   int L;                          // line length
   int S;                          // element stride of a line

@@ -23,6 +23,7 @@
 #include "fft_plan.hpp"
 #include "line_pass.cuh"
 #include "reduce.cuh"
+#include "stage_table.hpp"
 
 namespace qpb {
 
@@ -40,6 +41,7 @@ constexpr std::size_t kTwiddleOffset = 256;  // 3 axes x kNoAllocMaxLine float2
 constexpr std::size_t kAmpOffset = kTwiddleOffset + 3 * kNoAllocMaxLine * sizeof(float2);
 constexpr std::size_t kScratchBytes = kAmpOffset + kNoAllocMaxElements * sizeof(float);
 static_assert(sizeof(Ctrl) <= kCounterOffset, "control block overlaps the counter");
+static_assert(kNoAllocMaxLine >= 2 * 1024, "an axis slot holds W_L^k and the stage-major table");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -79,6 +81,14 @@ __global__ void twiddle_kernel(float2* tw, int length) {
     double s, c;
     sincospi(-2.0 * static_cast<double>(k) / static_cast<double>(length), &s, &c);
     tw[k] = {static_cast<float>(c), static_cast<float>(s)};
+  }
+}
+
+// The stage-major table of the register-resident passes (stage_table.hpp),
+// copied entry by entry from the W_L^k table `tw` (stream order makes it ready).
+__global__ void stage_twiddle_kernel(const float2* tw, float2* out, int length, StageGeometry g) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.count; i += gridDim.x * blockDim.x) {
+    out[i] = tw[stage_twiddle_exponent(g, length, i)];
   }
 }
 
@@ -162,6 +172,14 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
       p.amp = signed_amp;
       p.ctrl = ctrl;
       p.twiddle = tw;
+      p.stage_twiddle = tw;
+      const StageGeometry g = stage_geometry(L);
+      if (g.count > 0) {
+        // after the L entries of W_L^k in the axis's slot (L + count <= 2 L)
+        stage_twiddle_kernel<<<(g.count + 255) / 256, 256, 0, s>>>(tw, tw + L, L, g);
+        check_launch();
+        p.stage_twiddle = tw + L;
+      }
       p.n = n;
       p.L = L;
       p.S = a == 2 ? 1 : a == 1 ? dims[2] : dims[1] * dims[2];

@@ -19,7 +19,7 @@ struct ResidentParams {
   int starts_per_problem;
   const std::uint8_t* support;   // [starts][n]
   Ctrl* ctrl;                    // coefficients, error rows, counters[group] = first error row
-  const float2* twiddle;         // W_N^k, k < N
+  const float2* twiddle;         // stage-major table of the N-point transform (stage_table.hpp)
   int group;
   int start0;                    // first global start of the launch (error column)
   int starts_total;              // error row width

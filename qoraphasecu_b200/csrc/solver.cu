@@ -235,6 +235,7 @@ PassParams PassRunner::params(Mode mode, int axis3, int batch) const {
   p.stages = plan.stages;
   for (int s = 0; s < plan.stages; ++s) p.radix[s] = plan.radix[s];
   p.twiddle = plan.twiddle;
+  p.stage_twiddle = plan.stage_twiddle;
   p.scale = 1.0f / std::sqrt(static_cast<float>(p.n));
   p.amp_stride = 0;
   p.starts_per_problem = 1;
@@ -505,7 +506,7 @@ void Solver::enqueue_chunk(int len, cudaStream_t s) {
   p.starts_per_problem = spp_;
   p.support = support_.get();
   p.ctrl = ctrl_.get();
-  p.twiddle = runner_.params(Mode::kFwd, 2, starts_).twiddle;
+  p.twiddle = runner_.params(Mode::kFwd, 2, starts_).stage_twiddle;
   p.group = 0;
   p.start0 = 0;
   p.starts_total = starts_;
