@@ -248,6 +248,20 @@ def run_profile_step(sync_every, batch=0, schedule="auto"):
 
 
 # ----------------------------------------------------- the other synthetic workloads
+def tuned_batch(report):
+    """Starts per launch the autotuner chose for the benchmark shape and start
+    count (its report line "shape 1x256x256 starts 32 storage 0: batch 8 (...)"),
+    "resident" for the resident schedule, None when it has not run."""
+    key = f"shape 1x{SHAPE[0]}x{SHAPE[1]} starts {STARTS} storage 0: "
+    for line in report.splitlines():
+        if key in line:
+            choice = line.split(key, 1)[1]
+            if choice.startswith("batch "):
+                return int(choice.split()[1])
+            return "resident"
+    return None
+
+
 def _timed(fn, warmup=1, reps=3):
     """Median wall time of fn() after `warmup` calls (each call synchronises)."""
     for _ in range(warmup):
@@ -577,7 +591,7 @@ def main(argv=None):
             "starts_per_gpu": STARTS,
             "iterations": iters,
             "variant": "batched, graph-captured",
-            "starts_per_launch": args.batch or STARTS,
+            "starts_per_launch": args.batch or tuned_batch(qpc.api.tuning_report()),
             "sync_every": args.sync_every,
             "parallelism": f"replicas x{world}",
             "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write, outside step events)",

@@ -219,7 +219,9 @@ QPB_API uint64_t qpb_kernel_launches(void);
 QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
 
 /* Runs `iterations` more iterations with every line pass launched directly
- * between CUDA events on the solver's stream; ms_out[p] receives the mean
+ * between CUDA events on the solver's stream, all queued behind a short hold
+ * of the stream so that the device runs them back to back (the events time
+ * the kernels, not the host's launch rate); ms_out[p] receives the mean
  * duration of pass p of one iteration (2D: modulus pass, update pass; 3D adds
  * the y-axis inverse and forward passes) and *n_passes their count (<= 8).
  * With the resident schedule, *n_passes = 1 and ms_out[0] is the mean time per

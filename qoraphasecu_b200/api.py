@@ -440,7 +440,8 @@ class Solver:
 
     def profile_passes(self, iterations: int = 20):
         """Mean device time (ms) of each line pass of one iteration, timed with
-        CUDA events around direct launches; with the resident schedule, one
+        CUDA events around direct launches that the device runs back to back
+        (queued behind a short hold of the stream); with the resident schedule, one
         value: the mean time per iteration of one launch of ``iterations``
         iterations. Advances the iterate."""
         ms = (ctypes.c_double * 8)()

@@ -136,6 +136,18 @@ __global__ void scale_complex_kernel(float2* x, long long count, float scale) {
   QPB_FOR(i, count) { x[i] = cscale(x[i], scale); }
 }
 
+// Occupies the stream for about `ns` nanoseconds of the device's global
+// timer, sleeping between reads; at most 4096 sleeps of 1 us, so it ends.
+__global__ void hold_stream_kernel(long long ns) {
+  unsigned long long t0 = 0, t = 0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int i = 0; i < 4096; ++i) {
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (static_cast<long long>(t - t0) >= ns) break;
+    __nanosleep(1000);
+  }
+}
+
 dim3 grid(long long n, int batch) {
   return {static_cast<unsigned>(blocks_for(n)), static_cast<unsigned>(batch), 1};
 }
@@ -149,6 +161,12 @@ void random_wave(float2* w, const float* amplitude, long long amp_stride, int st
   random_wave_kernel<<<grid(n, batch), kThreads, 0, stream>>>(w, amplitude, amp_stride,
                                                               starts_per_problem, n, seed,
                                                               first_start);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+void hold_stream(long long ns, cudaStream_t stream) {
+  hold_stream_kernel<<<1, 32, 0, stream>>>(ns);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }

@@ -50,4 +50,9 @@ void set_ctrl(Ctrl* ctrl, const Ctrl& value, cudaStream_t stream);
 // x[b][i] = x[b][i] / scale (complex), used for results of scaled storage.
 void scale_complex(float2* x, long long count, float scale, cudaStream_t stream);
 
+// Keeps `stream` busy for about `ns` nanoseconds (at most about 4 ms), so that
+// the host can queue timed work behind it and the device then runs that work
+// back to back, its events timing the kernels rather than the host's launches.
+void hold_stream(long long ns, cudaStream_t stream);
+
 }  // namespace qpb

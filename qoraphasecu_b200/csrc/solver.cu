@@ -694,6 +694,9 @@ int Solver::profile_passes(int iterations, double* ms) {
   const int np = static_cast<int>(passes.size());
   std::vector<cudaEvent_t> events(static_cast<std::size_t>(2 * np * iterations));
   for (auto& e : events) QPB_CHECK(cudaEventCreate(&e));
+  // The host queues every launch and event while the stream is held, so the
+  // device runs them back to back and each event pair times its pass alone.
+  hold_stream(2000000, stream_);
   for (int it = 0; it < iterations; ++it) {
     for (int p = 0; p < np; ++p) {
       QPB_CHECK(cudaEventRecord(events[2 * (it * np + p)], stream_));
