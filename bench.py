@@ -62,16 +62,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def profile_value(key):
+    """The value of a `key: value` line in the committed ncu summaries, or None."""
     for f in sorted((ROOT / "profiles").glob("*.md")):
         for line in f.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch_update:"):
-                try:
-                    return float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    pass
+            if line.startswith(key + ":"):
+                return line.split(":", 1)[1].split()[0]
     return None
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` ("modulus" or "update") from the
+    committed ncu summary."""
+    value = profile_value(f"dram_bytes_per_launch_{kernel}")
+    try:
+        return float(value) if value is not None else None
+    except ValueError:
+        return None
 
 
 class ClockSampler:
@@ -540,13 +547,15 @@ def main(argv=None):
         unfused = UNFUSED_BYTES[name] * elems
         passes.append({"pass": name, "ms": ms, "bytes": bpe * elems, "gbs": bpe * elems / (ms * 1e6),
                        "unfused_equivalent_gbs": unfused / (ms * 1e6)})
-    # The dominant kernel is the update pass: the largest share of the step's
-    # device time in the ncu launch list (49% against the modulus pass's 48%);
-    # their single-launch times are within noise of each other, so picking the
-    # larger of two measured times would flip between runs. Both are reported.
-    dominant = passes[1]
+    # The dominant kernel is the pass with the largest share of the step's
+    # device time in the committed ncu launch list (its `dominant_kernel:`
+    # line); the two passes' shares and single-launch times are close, so
+    # picking the larger of two measured times would flip between runs. Both
+    # passes are reported.
+    dominant_name = profile_value("dominant_kernel") or "modulus"
+    dominant = passes[0] if dominant_name == "modulus" else passes[1]
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(dominant_name)
     # The whole iteration in the timed graph (parallel start groups, shrinkwrap
     # amortised): the minimum 21 B per element per iteration (iterate in and
     # out, amplitude, support) and the bytes the two fused passes move.
