@@ -321,7 +321,7 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   x_ = DeviceBuffer<float2>(total);
   w_ = DeviceBuffer<float2>(total);
   saved_ = DeviceBuffer<std::uint8_t>(total);
-  level_ = DeviceBuffer<LevelAcc>(static_cast<std::size_t>(batch_));
+  level_ = DeviceBuffer<LevelAcc>(static_cast<std::size_t>(starts_));
   moments_ = DeviceBuffer<unsigned long long>(2 * static_cast<std::size_t>(starts_));
   ctrl_ = DeviceBuffer<Ctrl>(1);
   counters_ = DeviceBuffer<int>(static_cast<std::size_t>(groups_));
@@ -727,21 +727,26 @@ void Solver::shrinkwrap(const OpDesc& o) {
   const float half_pi = kTwoPi / 2;
   const float k = -2.0f * half_pi * half_pi * o.sigma * o.sigma;
   const int outer = runner_.outer();
-  for (int g = 0; g < groups_; ++g) {
-    QPB_CHECK(cudaMemsetAsync(level_.get(), 0, batch_ * sizeof(LevelAcc), stream_));
-    PassParams first = base(Mode::kBlurMag, outer, g);
-    first.blur_k = k;
-    runner_.launch(Mode::kBlurMag, outer, first, stream_);
-    if (runner_.has_mid()) {
-      PassParams mid = base(Mode::kBlur, 1, g);
-      mid.blur_k = k;
-      runner_.launch(Mode::kBlur, 1, mid, stream_);
-    }
-    PassParams last = base(Mode::kBlur, 2, g);
-    last.blur_k = k;
+  // A batched solver blurs every start in one launch per axis (one level
+  // accumulator per start), whatever its start groups; the plain variant
+  // keeps one start per launch like the rest of its iteration.
+  const bool together = options_.variant == Variant::kBatched;
+  const int chunks = together ? 1 : groups_;
+  const int count = together ? starts_ : batch_;
+  auto params = [&](Mode mode, int axis3, int g) {
+    PassParams p = base(mode, axis3, g);
+    p.lines = runner_.params(mode, axis3, count).lines;
+    p.blur_k = k;
+    return p;
+  };
+  for (int g = 0; g < chunks; ++g) {
+    QPB_CHECK(cudaMemsetAsync(level_.get(), 0, count * sizeof(LevelAcc), stream_));
+    runner_.launch(Mode::kBlurMag, outer, params(Mode::kBlurMag, outer, g), stream_);
+    if (runner_.has_mid()) runner_.launch(Mode::kBlur, 1, params(Mode::kBlur, 1, g), stream_);
+    PassParams last = params(Mode::kBlur, 2, g);
     last.level_method = o.method + 1;
     runner_.launch(Mode::kBlur, 2, last, stream_);
-    shrinkwrap_threshold(w(g), level_.get(), n_, batch_, o.method + 1, o.threshold, support(g),
+    shrinkwrap_threshold(w(g), level_.get(), n_, count, o.method + 1, o.threshold, support(g),
                          stream_);
   }
   wave_valid_ = false;

@@ -9,10 +9,11 @@
 // CTAs run with the SMs half idle; several smaller groups become parallel
 // branches of the captured graph, and one group's modulus pass then overlaps
 // another's update pass. The best choice depends on the shape, the start count
-// and the device, so it is measured: each candidate runs a short RAAR stage on
-// a scratch solver built from the same problem, and the fastest is cached for
-// the process.
+// and the device, so it is measured: each candidate runs a short RAAR stage
+// (two chunks of the caller's length) on a scratch solver built from the same
+// problem, and the fastest is cached for the process.
 
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <map>
@@ -50,13 +51,16 @@ double time_candidate(const ProblemView& problem, const SolverOptions& base, int
   o.start = nullptr;
   o.seed = 0;
   o.stream = nullptr;
-  o.sync_every = 10;
+  // The caller's chunk length (10..100 iterations), so that each candidate
+  // replays the graphs the caller's run would replay; two chunks per timing
+  // keep the host's share of the wall time small.
+  o.sync_every = std::max(10, std::min(base.sync_every, 100));
   o.variant = Variant::kBatched;
   Solver solver(problem, o);
-  const OpDesc raar{kOpRAAR, 10, 0.9f, 0.0f, 0.0f, 0, 0};
+  const OpDesc raar{kOpRAAR, 2 * o.sync_every, 0.9f, 0.0f, 0.0f, 0, 0};
   solver.run(&raar, 1);  // captures the graph
   double best = 1e30;
-  for (int rep = 0; rep < 2; ++rep) {
+  for (int rep = 0; rep < 3; ++rep) {
     const auto t0 = std::chrono::steady_clock::now();
     solver.run(&raar, 1);
     const auto t1 = std::chrono::steady_clock::now();
