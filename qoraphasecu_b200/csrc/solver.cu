@@ -476,13 +476,25 @@ PassParams Solver::base(Mode mode, int axis3, int g) const {
   return p;
 }
 
-void Solver::enqueue_establish(int g) {
-  runner_.launch(Mode::kFwdFromX, 2, base(Mode::kFwdFromX, 2, g), stream_);
-  if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+void Solver::enqueue_establish(int g, int count) {
+  PassParams first = base(Mode::kFwdFromX, 2, g);
+  first.lines = runner_.params(Mode::kFwdFromX, 2, count).lines;
+  runner_.launch(Mode::kFwdFromX, 2, first, stream_);
+  if (runner_.has_mid()) {
+    PassParams mid = base(Mode::kFwd, 1, g);
+    mid.lines = runner_.params(Mode::kFwd, 1, count).lines;
+    runner_.launch(Mode::kFwd, 1, mid, stream_);
+  }
 }
 
+// A batched solver's starts in one launch per axis, whatever its groups; the
+// plain variant one start per launch like the rest of its iteration.
 void Solver::establish_wave() {
-  for (int g = 0; g < groups_; ++g) enqueue_establish(g);
+  if (options_.variant == Variant::kBatched) {
+    enqueue_establish(0, starts_);
+  } else {
+    for (int g = 0; g < groups_; ++g) enqueue_establish(g, batch_);
+  }
   wave_valid_ = true;
 }
 

@@ -268,7 +268,8 @@ class Solver {
   void load(const std::vector<ProblemView>& problems, std::uint64_t seed, const float2* start);
   void enqueue_iteration(int g, cudaStream_t s);
   void enqueue_chunk(int len, cudaStream_t s);  // resident: `len` iterations in one launch
-  void enqueue_establish(int g);
+  // w = FFT_inner(x) for `count` starts from group g's first one
+  void enqueue_establish(int g, int count);
   void establish_wave();
   void iterate(int count, Coefficients c);
   void shrinkwrap(const OpDesc& o);
