@@ -410,9 +410,13 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   set_ctrl(ctrl_.get(), ctrl, stream_);
   for (int q = 0; q < problems_; ++q) {
     std::uint8_t* first = support_.get() + static_cast<std::size_t>(q) * spp_ * n_;
-    for (int s = 1; s < spp_; ++s) {
-      QPB_CHECK(cudaMemcpyAsync(first + static_cast<std::size_t>(s) * n_, first,
-                                static_cast<std::size_t>(n_), cudaMemcpyDeviceToDevice, stream_));
+    // the first start's support to the others, doubling the copied block
+    for (int have = 1; have < spp_;) {
+      const int take = std::min(have, spp_ - have);
+      QPB_CHECK(cudaMemcpyAsync(first + static_cast<std::size_t>(have) * n_, first,
+                                static_cast<std::size_t>(take) * n_, cudaMemcpyDeviceToDevice,
+                                stream_));
+      have += take;
     }
   }
   stream_.sync();
@@ -431,19 +435,30 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   } else {
     // Random phases on the measured amplitude, inverse transform, cut to the
     // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
-    for (int g = 0; g < groups_; ++g) {
-      random_wave(w(g), amp_f_.get(), amp_stride_, spp_, n_, batch_, seed,
+    // A batched solver draws every start in one launch per pass (each start
+    // keyed by its global index, as in its own group); the plain variant one
+    // start per launch.
+    const bool together = options_.variant == Variant::kBatched;
+    const int chunks = together ? 1 : groups_;
+    const int count = together ? starts_ : batch_;
+    auto params = [&](Mode mode, int axis3, int g) {
+      PassParams p = base(mode, axis3, g);
+      p.lines = runner_.params(mode, axis3, count).lines;
+      return p;
+    };
+    for (int g = 0; g < chunks; ++g) {
+      random_wave(w(g), amp_f_.get(), amp_stride_, spp_, n_, count, seed,
                   static_cast<std::uint64_t>(g) * batch_, stream_);
       const int outer = runner_.outer();
-      runner_.launch(Mode::kInv, outer, base(Mode::kInv, outer, g), stream_);
-      if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, base(Mode::kInv, 1, g), stream_);
-      PassParams u = base(Mode::kUpd, 2, g);
+      runner_.launch(Mode::kInv, outer, params(Mode::kInv, outer, g), stream_);
+      if (runner_.has_mid()) runner_.launch(Mode::kInv, 1, params(Mode::kInv, 1, g), stream_);
+      PassParams u = params(Mode::kUpd, 2, g);
       u.coef_from_ctrl = 0;
       u.coef_a = 0.0f;
       u.coef_b = 0.0f;
       u.bump_counter = 0;
       runner_.launch(Mode::kUpd, 2, u, stream_);
-      if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, base(Mode::kFwd, 1, g), stream_);
+      if (runner_.has_mid()) runner_.launch(Mode::kFwd, 1, params(Mode::kFwd, 1, g), stream_);
     }
     wave_valid_ = true;
   }
