@@ -84,7 +84,7 @@ TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& op
   if (auto it = g_choice.find(key); it != g_choice.end()) return it->second;
   std::vector<int> candidates;
   if (resident_ok) candidates.push_back(0);
-  for (int parts : {1, 2, 4, 8}) {
+  for (int parts : {1, 2, 4, 8, 16}) {
     if (starts % parts == 0 && starts / parts >= 1) candidates.push_back(starts / parts);
   }
   TunedSchedule best{starts, false};
