@@ -44,16 +44,19 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 // 69.6 us with 32 lines and 62.6 us with 4). Rows of 512 and 1024 points take
 // one line per CTA, budgeted 128 registers a thread (their three-stage
 // transforms spill at 80): a 512^2 update pass of 16 starts measured 29.6 us
-// against 39.4 us with 16 lines per CTA and 30.8 us with 2. Columns keep
-// 256 / T lines up to 256 points (16 at 256, and at 512), whose 128-byte and
-// longer row segments load better (fewer columns per CTA measured slower: 8
-// at 512 took 37.2 us against 35.2 us).
+// against 39.4 us with 16 lines per CTA and 30.8 us with 2. Columns of 128
+// points take 16 lines (128 threads; the 128^3 z-axis modulus pass measured
+// 42 us against 47 us with 32 lines); other columns keep 256 / T lines up
+// to 256 points (16 at 256, and at 512), whose 128-byte and longer row
+// segments load better (fewer columns per CTA measured slower: 8 at 512 took
+// 37.2 us against 35.2 us, 8 at 128 ran the 128^3 workload 17% slower).
 template <int L, bool ROWS>
 struct Tiling {
   using G = Geometry<L>;
   static constexpr int LINES = (ROWS && L >= 512)   ? 1
                                : (ROWS && L == 256) ? 4
                                : (ROWS && L == 128) ? 8
+                               : (!ROWS && L == 128) ? 16
                                                     : (G::T <= 16 ? 256 / G::T : (L >= 1024 ? 8 : 16));
   static constexpr int NT = G::T * LINES;
   static constexpr int MIN_CTAS = L >= 512 ? (NT < 512 ? 512 / NT : 1)
