@@ -136,17 +136,47 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference arm
-def reference_sample(problem_arrays, starts, iterations, threads, port=False):
-    """Times `iterations` RAAR iterations of `starts` starts on the host CPU with
-    the reference's own CpuSolver (compiled from its sources) when available
-    and `port` is false, else the oracle's numpy port of CpuSolver::iterate on
-    scipy.fft (pocketfft C++). Returns (seconds, kind, label)."""
-    intensity, mask = problem_arrays
+# A CPU step is the whole benchmark recipe (RAAR + Shrinkwrap + ER, 700
+# iterations) on a sample of the 32 starts: starts 0..CPU_SAMPLE_STARTS-1,
+# drawn exactly as the GPU arm draws its starts 0..3. The reference's CpuSolver
+# runs the starts of a step one after another, each on every host thread, so
+# the sample's rate per start-iteration is the whole job's.
+CPU_SAMPLE_STARTS = 4
+PORT_SAMPLE_STARTS = 2
+
+
+def config_of(args, world):
+    """The workload description both arms print (the arm-specific schedule and
+    sampling are reported beside it)."""
+    return {
+        "workload": WORKLOAD,
+        "shape": list(SHAPE),
+        "starts_per_gpu": STARTS,
+        "iterations": 700,
+        "parallelism": f"replicas x{world}",
+        "l2": f"GPU arm: {L2_FLUSH_BYTES >> 20} MiB write between steps, outside the step events; "
+              "CPU arm: n/a",
+    }
+
+
+def reference_step(intensity, mask, starts, threads, port=False):
+    """One CPU step: the whole recipe on `starts` starts with the reference's
+    own CpuSolver (compiled from its sources) when available and `port` is
+    false, else the oracle's numpy port of CpuSolver::iterate on scipy.fft
+    (pocketfft C++). Solver construction is not timed. Returns (seconds, kind,
+    label)."""
+    from qoraphasecu_b200 import workloads
+
+    recipe = workloads.gaussians_recipe().ops()
     from oracle import ref as oracle_ref
 
     if not port and oracle_ref.available():
-        seconds = oracle_ref.time_iterations(intensity, mask, starts, iterations, threads)
-        return seconds, "reference", "QoraPhaseCU CpuSolver (OpenMP loops, project FFT shim)"
+        oracle_ref.load().qref_set_threads(threads)
+        problem = oracle_ref.make_problem(intensity, None, mask)
+        solver = oracle_ref.Solver(problem, starts=starts, seed=0)
+        t0 = time.perf_counter()
+        solver.run(recipe)
+        return time.perf_counter() - t0, "reference", "QoraPhaseCU CpuSolver (OpenMP loops, project FFT shim)"
     import numpy as np
 
     from oracle import fp64
@@ -154,23 +184,23 @@ def reference_sample(problem_arrays, starts, iterations, threads, port=False):
     problem = fp64.make_problem(intensity, None, mask)
     solver = fp64.Solver(problem, starts=starts, dtype=np.complex64, fft="scipy", workers=threads)
     t0 = time.perf_counter()
-    solver.run([fp64.op("raar", iterations, 0.9)])
+    solver.run(recipe)
     return time.perf_counter() - t0, "port", "numpy port of CpuSolver::iterate, scipy.fft (pocketfft)"
 
 
-def cpu_baseline(intensity, mask, budget_s=10.0, port=False):
+def cpu_baseline(intensity, mask, port=False):
+    """The CPU figure beside the GPU line: one untimed step, then one timed step."""
     threads = len(os.sched_getaffinity(0))
-    iters = 2
-    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads, port)
-    # grow the sample to about `budget_s` of CPU work
-    iters = max(2, min(200, int(iters * budget_s / max(seconds, 1e-3))))
-    seconds, kind, label = reference_sample((intensity, mask), STARTS, iters, threads, port)
+    starts = PORT_SAMPLE_STARTS if port else CPU_SAMPLE_STARTS
+    reference_step(intensity, mask, starts, threads, port)
+    seconds, kind, label = reference_step(intensity, mask, starts, threads, port)
     return {
-        "value": STARTS * iters / seconds,
+        "value": starts * 700 / seconds,
         "unit": UNIT,
         "cores": threads,
         "kind": kind,
-        "sample": f"{STARTS} starts x {iters} RAAR iterations at 256x256 ({label}), {seconds:.1f} s",
+        "sample": f"the whole 700-iteration recipe on {starts} of the 32 starts ({label}), "
+                  f"{seconds:.2f} s",
     }
 
 
@@ -181,13 +211,17 @@ def run_reference(args):
     from qoraphasecu_b200 import workloads
 
     _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
+    threads = len(os.sched_getaffinity(0))
     for _ in range(args.warmup):
-        pass  # the sample itself warms up (first call builds FFT plans)
-    samples = []
+        reference_step(intensity, mask, CPU_SAMPLE_STARTS, threads)
+    seconds = []
     for _ in range(args.steps):
-        samples.append(cpu_baseline(intensity, mask, budget_s=args.cpu_seconds))
-    value = statistics.median(s["value"] for s in samples)
-    base = samples[-1]
+        t, kind, label = reference_step(intensity, mask, CPU_SAMPLE_STARTS, threads)
+        seconds.append(t)
+    total = sum(seconds)
+    value = CPU_SAMPLE_STARTS * 700 * args.steps / total
+    sample = (f"each step: the whole 700-iteration recipe on starts 0-{CPU_SAMPLE_STARTS - 1} of "
+              f"the 32 ({label}); {args.steps} steps in {total:.1f} s")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -196,18 +230,102 @@ def run_reference(args):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 * STARTS * 700 / value,
+        "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded gaussians generator)",
-        "config": {"workload": WORKLOAD, "l2": "n/a (host CPU)"},
-        "cpu_baseline": {**base, "value": value},
+        "data": "synthetic (seeded gaussians generator, seed 1000; random starts seed 0)",
+        "config": config_of(args, args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+REFERENCE_GPU_VARIANTS = {"graph": 2, "batched": 3, "half": 4, "mixed": 6}  # qpcu::Variant
+
+
+def reference_gpu_baseline(intensity, mask, sync_every):
+    """The reference's own CUDA backend (src/cuda: cuFFT plans, its element-wise
+    kernels, CUDA graphs) compiled from its sources (oracle/_ref/
+    libqpcu_ref_cuda.so, cuFFT LTO callbacks off) on the same workload, timed
+    as its bench/bench.cpp:33-45 does: per variant, one run of the whole recipe
+    to warm up (plans, graphs), then one timed run, wall clock around run()
+    (which ends with the errors copied to the host)."""
+    import ctypes
+
+    import numpy as np
+
+    from oracle import ref as oracle_ref
+    from qoraphasecu_b200 import workloads
+
+    if not oracle_ref.CUDA_LIBRARY.exists():
+        return {"unavailable": "oracle/_ref/libqpcu_ref_cuda.so was not built"}
+    lib = oracle_ref.load_variant("cuda")
+    if not lib.qref_cuda_available():
+        return {"unavailable": "no CUDA device"}
+    amp, msk, sup = oracle_ref.make_problem(intensity, None, mask)
+    ops = oracle_ref._ops(workloads.gaussians_recipe().ops())
+    count = len(workloads.gaussians_recipe().ops())
+    out = {"source": "QoraPhaseCU src/cuda compiled from its sources (nvcc sm_100a, cuFFT "
+                     "11.4, LTO callbacks off)", "starts": STARTS, "sync_every": sync_every}
+    for name, variant in REFERENCE_GPU_VARIANTS.items():
+        handle = ctypes.c_void_p()
+        status = lib.qref_create_backend(oracle_ref._p(amp), oracle_ref._p(msk),
+                                         oracle_ref._p(sup), 2, oracle_ref._shape(amp.shape),
+                                         STARTS, ctypes.c_uint64(0), None, sync_every, 1,
+                                         variant, 0, ctypes.byref(handle))
+        if status:
+            out[name] = {"error": lib.qref_last_error().decode()}
+            continue
+        try:
+            if lib.qref_run(handle, ops, count):
+                out[name] = {"error": lib.qref_last_error().decode()}
+                continue
+            t0 = time.perf_counter()
+            status = lib.qref_run(handle, ops, count)
+            seconds = time.perf_counter() - t0
+            if status:
+                out[name] = {"error": lib.qref_last_error().decode()}
+                continue
+            n_err = lib.qref_error_count(handle)
+            errors = np.empty((STARTS, n_err), np.float32)
+            lib.qref_results(handle, None, None, oracle_ref._p(errors),
+                             ctypes.byref(ctypes.c_size_t()))
+            out[name] = {"value": STARTS * 700 / seconds, "unit": UNIT,
+                         "us_per_iteration": seconds / 700 * 1e6,
+                         "best_final_error": float(errors[:, -1].min())}
+        finally:
+            lib.qref_destroy(handle)
+    return out
+
+
+def parity_check(solver_kwargs, intensity, mask):
+    """RAAR(0.9) x 2 from the timed solver's starts against the FP64 oracle
+    (outside any timed region): the largest relative difference of the
+    per-iteration Fourier errors and the largest relative L2 difference of the
+    objects over all 32 starts."""
+    import numpy as np
+
+    import qoraphasecu_b200 as qpc
+    from oracle import fp64
+    from qoraphasecu_b200.recipe import RAAR, Recipe
+
+    problem = qpc.make_problem(intensity, mask=mask)
+    with qpc.Solver(problem, **solver_kwargs) as s:
+        s.run(Recipe(RAAR(2, 0.9)))
+        ours = s.results()
+    ref = fp64.reconstruct(fp64.make_problem(intensity, None, mask), [fp64.op("raar", 2, 0.9)],
+                           starts=solver_kwargs["starts"], seed=solver_kwargs["seed"])
+    err = max(float(np.max(np.abs(r.errors - e) / e)) for r, (_, _, e) in zip(ours, ref))
+    obj = max(fp64.relative_diff(r.object, o) for r, (o, _, _) in zip(ours, ref))
+    return {"recipe": "RAAR(0.9) x 2, all 32 starts, the timed solver's options",
+            "against": "FP64 oracle (numpy complex128 restatement of CpuSolver)",
+            "error_rel_max": err, "object_rel_l2_max": obj, "bar": 1e-5,
+            "ok": bool(err < 1e-5 and obj < 1e-5)}
 
 
 def run_profile(iterations, schedule="streamed"):
@@ -449,7 +567,6 @@ def main(argv=None):
     parser.add_argument("--sync-every", type=int, default=50)
     parser.add_argument("--batch", type=int, default=0,
                         help="starts per launch; groups run as parallel graph branches (0 = all)")
-    parser.add_argument("--cpu-seconds", type=float, default=10.0)
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
     parser.add_argument("--profile", type=int, default=0, metavar="ITERS",
@@ -507,9 +624,10 @@ def main(argv=None):
     iters = recipe.iterations()
     stream = torch.cuda.current_stream()
     problem = qpc.make_problem(intensity, mask=mask)
-    solver = qpc.Solver(problem, starts=STARTS, seed=seed, sync_every=args.sync_every,
-                        batch=args.batch or None, device=local, stream=stream.cuda_stream,
-                        schedule=args.schedule)
+    solver_kwargs = dict(starts=STARTS, seed=seed, sync_every=args.sync_every,
+                         batch=args.batch or None, device=local, stream=stream.cuda_stream,
+                         schedule=args.schedule)
+    solver = qpc.Solver(problem, **solver_kwargs)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
@@ -570,6 +688,8 @@ def main(argv=None):
         "unit": "GB/s",
         "frac": dominant["gbs"] / peak,
         "traffic": traffic,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, from the "
+                          "committed summary under profiles/ (not measured in this run)",
         "passes": passes,
         "iteration": {
             "us": iter_ms * 1e3,
@@ -594,16 +714,11 @@ def main(argv=None):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded gaussians generator, seed 1000; random starts seed = rank)",
-        "config": {
-            "workload": WORKLOAD,
-            "shape": list(SHAPE),
-            "starts_per_gpu": STARTS,
-            "iterations": iters,
+        "config": config_of(args, world),
+        "schedule": {
             "variant": "batched, graph-captured",
             "starts_per_launch": args.batch or tuned_batch(qpc.api.tuning_report()),
             "sync_every": args.sync_every,
-            "parallelism": f"replicas x{world}",
-            "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write, outside step events)",
         },
         "gpu_launches": launches,
         "tuning": qpc.api.tuning_report().strip().splitlines(),
@@ -673,12 +788,16 @@ def main(argv=None):
 
     line["clocks"] = clocks.summary()
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(intensity, mask, budget_s=args.cpu_seconds)
+        # The CPU leg, after every timed region: the reference's CPU path as the
+        # baseline, and the FP64 oracle as the checker of the timed solver's
+        # first two iterations.
+        line["cpu_baseline"] = cpu_baseline(intensity, mask)
         if line["cpu_baseline"]["kind"] == "reference":
-            # the second CPU figure: the same iteration on pocketfft (scipy.fft),
+            # the second CPU figure: the same recipe on pocketfft (scipy.fft),
             # the FFT the reference's CPU backend links
-            line["cpu_baseline_pocketfft"] = cpu_baseline(intensity, mask,
-                                                          budget_s=args.cpu_seconds, port=True)
+            line["cpu_baseline_pocketfft"] = cpu_baseline(intensity, mask, port=True)
+        line["parity"] = parity_check(solver_kwargs, intensity, mask)
+        line["reference_gpu_baseline"] = reference_gpu_baseline(intensity, mask, args.sync_every)
     solver.close()
     if dist:
         dist.barrier()

@@ -41,8 +41,20 @@ typedef enum qpb_amp_storage { QPB_AMP_F32 = 0, QPB_AMP_F16 = 1, QPB_AMP_BF16 = 
 
 /* Execution schedule. BATCHED runs `batch` starts per launch with iterations
  * replayed from CUDA graphs; PLAIN runs one start per launch, launched
- * directly (the in-repo baseline). Replaces qpcu::Variant (solver.hpp:21-29). */
-typedef enum qpb_variant { QPB_VARIANT_BATCHED = 0, QPB_VARIANT_PLAIN = 1 } qpb_variant;
+ * directly (the in-repo baseline). HALF and MIXED are BATCHED with fp16
+ * storage, the reference's Variant::half and Variant::mixed
+ * (src/cuda/half.cu:14-83, cuda_solver.cu:74-86): HALF stores the iterate and
+ * the wave as fp16 pairs; MIXED stores the wave in fp16 during HIO and RAAR,
+ * runs ER entirely in FP32 and keeps an FP32 iterate. Both divide the
+ * amplitude by its peak (objects are returned in the data's scale), compute
+ * in FP32, need power-of-two extents of 16..1024 and an FP32 amplitude, and run
+ * the streamed schedule. Replaces qpcu::Variant (solver.hpp:21-29). */
+typedef enum qpb_variant {
+  QPB_VARIANT_BATCHED = 0,
+  QPB_VARIANT_PLAIN = 1,
+  QPB_VARIANT_HALF = 2,
+  QPB_VARIANT_MIXED = 3
+} qpb_variant;
 
 /* How BATCHED iterations run (no counterpart in the reference). STREAMED: two
  * line passes per 2D iteration (four in 3D) through HBM, start groups as
@@ -193,6 +205,17 @@ QPB_API qpb_status qpb_run(qpb_solver* solver, const qpb_op* ops, size_t n_ops);
 QPB_API qpb_status qpb_reset(qpb_solver* solver, const qpb_problem* problems, size_t n_problems,
                              uint64_t seed, const float* start);
 
+/* Bounded waits (no counterpart in the reference, whose kernels never wait on
+ * one another). The line passes stage inputs by asynchronous bulk copies and
+ * wait for them a bounded number of polls (about 4 million by default); a CTA
+ * that gives up writes nothing and counts itself in a counter of the solver,
+ * and the qpb_run that launched it returns QPB_TIMEOUT. `polls` sets the limit
+ * for the launches that follow (captured graphs are re-captured). `starve`
+ * non-zero is fault injection for tests of that path: the staged copies are
+ * left out, so every staged wait runs out; results are invalid until the
+ * solver is reset with starve 0 and qpb_reset. */
+QPB_API qpb_status qpb_set_wait_limit(qpb_solver* solver, int polls, int starve);
+
 /* Progress callback (Options::progress, solver.hpp:52-54); NULL disables it. */
 QPB_API qpb_status qpb_set_progress(qpb_solver* solver, qpb_progress_fn fn, void* user);
 
@@ -244,8 +267,14 @@ QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double
  * return QPB_INVALID_ARGUMENT. The first call on a device looks up the array's
  * device address and configures kernels; make that first call before any
  * stream capture. All calls on a device share the array, which keeps the last
- * call's contents (each call clears what must start at zero): calls that
- * overlap on the GPU, e.g. on two streams, race on it. */
+ * call's contents (each call clears what must start at zero; the twiddle
+ * tables of the previous shape are reused): calls that overlap on the GPU,
+ * e.g. on two streams, race on it.
+ *   x and out must be 16-byte aligned (they are moved by bulk copies), the
+ * amplitude and error_out 4-byte aligned; a misaligned pointer returns
+ * QPB_INVALID_ARGUMENT before anything is launched. If a line pass gives up a
+ * bounded wait for its staged inputs, *error_out is NaN and out is not the
+ * projection. */
 QPB_API qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape,
                                                const float* amplitude, const uint8_t* mask,
                                                const float* x, float* out, float* error_out,
@@ -263,7 +292,10 @@ QPB_API qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape,
  * Enqueued on `stream` (cudaStream_t; NULL = legacy default stream); returns
  * without waiting. The first call per device and shape builds line plans
  * (device allocations kept for the process); calls on one device share a
- * control block, so calls that overlap on the GPU race. */
+ * control block, so calls that overlap on the GPU race. signed_amplitude, x
+ * and grad must be 16-byte aligned (bulk copies move them), loss 8-byte
+ * aligned; otherwise QPB_INVALID_ARGUMENT. If a line pass gives up a bounded
+ * wait for its staged inputs, every loss is NaN. */
 QPB_API qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int batch,
                                            const float* signed_amplitude, const float* x,
                                            float* grad, double* loss, void* stream);

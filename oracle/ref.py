@@ -18,9 +18,11 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "_ref" / "libqpcu_ref.so"
-REFERENCE = Path(os.environ.get("QPCU_REFERENCE", "/root/reference"))
+CUDA_LIBRARY = HERE / "_ref" / "libqpcu_ref_cuda.so"
+DROPIN_LIBRARY = HERE / "_ref" / "libqpcu_dropin.so"
 
 _lib = None
+_libs = {}
 
 OP_KINDS = {"er": 0, "hio": 1, "raar": 2, "shrinkwrap": 3, "detwin_begin": 4, "detwin_end": 5}
 
@@ -30,11 +32,14 @@ class _Op(ctypes.Structure):
                 ("sigma", c_float), ("method", c_int), ("axis", c_int)]
 
 
-def build() -> bool:
-    """Compiles the reference oracle when the reference sources are present."""
-    if not (REFERENCE / "src" / "cpu" / "cpu_solver.cpp").exists():
+def build(reference=None) -> bool:
+    """Compiles the reference oracle libraries (oracle/Makefile) when the
+    reference sources are present at `reference` (default: the QPCU_REFERENCE
+    environment variable); without them, the libraries built before are kept."""
+    root = reference or os.environ.get("QPCU_REFERENCE")
+    if not root or not (Path(root) / "src" / "cpu" / "cpu_solver.cpp").exists():
         return LIBRARY.exists()
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE}"], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={root}", "all"], check=True)
     return LIBRARY.exists()
 
 
@@ -42,26 +47,49 @@ def available() -> bool:
     return LIBRARY.exists()
 
 
+def _configure(lib):
+    lib.qref_last_error.restype = c_char_p
+    lib.qref_set_threads.argtypes = [c_int]
+    lib.qref_set_threads.restype = None
+    lib.qref_create.argtypes = [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int64), c_int,
+                                c_uint64, c_void_p, c_int, POINTER(c_void_p)]
+    lib.qref_create_backend.argtypes = [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int64),
+                                        c_int, c_uint64, c_void_p, c_int, c_int, c_int, c_int,
+                                        POINTER(c_void_p)]
+    lib.qref_reconstruct.argtypes = [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int64),
+                                     c_void_p, c_size_t, c_int, c_uint64, c_int, c_void_p,
+                                     c_void_p, c_void_p, POINTER(c_int)]
+    lib.qref_cuda_available.restype = c_int
+    lib.qref_run.argtypes = [c_void_p, c_void_p, c_size_t]
+    lib.qref_results.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_size_t)]
+    lib.qref_error_count.argtypes = [c_void_p]
+    lib.qref_error_count.restype = c_size_t
+    lib.qref_destroy.argtypes = [c_void_p]
+    lib.qref_destroy.restype = None
+    for name in ("qref_fft", "qref_make_problem", "qref_modulus_project", "qref_gaussian_blur",
+                 "qref_half_support", "qref_autocorrelation_support",
+                 "qref_simulate_intensity", "qref_aligned_error"):
+        getattr(lib, name).restype = c_int
+    return lib
+
+
+def load_variant(which: str):
+    """One of the oracle libraries: "cpu" (the reference's CPU path), "cuda"
+    (plus the reference's own CUDA backend) or "dropin" (the reference's core
+    with its Backend::cuda slot bound to the B200 adapter)."""
+    path = {"cpu": LIBRARY, "cuda": CUDA_LIBRARY, "dropin": DROPIN_LIBRARY}[which]
+    if which not in _libs:
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is missing: build it with oracle/Makefile")
+        _libs[which] = _configure(ctypes.CDLL(str(path)))
+    return _libs[which]
+
+
 def load():
+    """The reference's CPU path (oracle/_ref/libqpcu_ref.so)."""
     global _lib
     if _lib is None:
-        lib = ctypes.CDLL(str(LIBRARY))
-        lib.qref_last_error.restype = c_char_p
-        lib.qref_set_threads.argtypes = [c_int]
-        lib.qref_set_threads.restype = None
-        lib.qref_create.argtypes = [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int64), c_int,
-                                    c_uint64, c_void_p, c_int, POINTER(c_void_p)]
-        lib.qref_run.argtypes = [c_void_p, c_void_p, c_size_t]
-        lib.qref_results.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_size_t)]
-        lib.qref_error_count.argtypes = [c_void_p]
-        lib.qref_error_count.restype = c_size_t
-        lib.qref_destroy.argtypes = [c_void_p]
-        lib.qref_destroy.restype = None
-        for name in ("qref_fft", "qref_make_problem", "qref_modulus_project", "qref_gaussian_blur",
-                     "qref_half_support", "qref_autocorrelation_support",
-                     "qref_simulate_intensity", "qref_aligned_error"):
-            getattr(lib, name).restype = c_int
-        _lib = lib
+        _lib = load_variant("cpu")
     return _lib
 
 

@@ -195,6 +195,59 @@ int qref_create(const float* amp, const uint8_t* mask, const uint8_t* support, i
   });
 }
 
+// qref_create with the backend (0 cpu, 1 cuda: whatever the library binds
+// there), the variant (qpcu::Variant, used by the reference's CUDA backend)
+// and the starts per batched plan.
+int qref_create_backend(const float* amp, const uint8_t* mask, const uint8_t* support, int ndim,
+                        const int64_t* shape, int starts, uint64_t seed, const float* start,
+                        int sync_every, int backend, int variant, int batch, void** out) {
+  return guarded([&] {
+    auto p = problem_of(amp, mask, support, ndim, shape);
+    qpcu::Options o;
+    o.backend = backend == 1 ? qpcu::Backend::cuda : qpcu::Backend::cpu;
+    o.variant = static_cast<qpcu::Variant>(variant);
+    o.batch = batch;
+    o.starts = starts;
+    o.seed = seed;
+    o.sync_every = sync_every;
+    if (start) {
+      const auto* c = reinterpret_cast<const qpcu::Complex*>(start);
+      o.start.assign(c, c + qpcu::numel(p.shape) * static_cast<std::size_t>(starts));
+    }
+    auto* r = new RefSolver{p.shape, qpcu::make_solver(p, o)};
+    *out = r;
+  });
+}
+
+// qpcu::reconstruct (src/core/solver.cpp:88-93) and qpcu::best_index
+// (:95-103) through the reference's public API on a made problem; outputs as
+// qref_results, *best the index best_index picks.
+int qref_reconstruct(const float* amp, const uint8_t* mask, const uint8_t* support, int ndim,
+                     const int64_t* shape, const void* ops, size_t count, int starts, uint64_t seed,
+                     int backend, float* objects, uint8_t* supports, float* errors, int* best) {
+  return guarded([&] {
+    const auto p = problem_of(amp, mask, support, ndim, shape);
+    qpcu::Options o;
+    o.backend = backend == 1 ? qpcu::Backend::cuda : qpcu::Backend::cpu;
+    o.starts = starts;
+    o.seed = seed;
+    const auto runs = qpcu::reconstruct(p, recipe_of(static_cast<const Op*>(ops), count), o);
+    const std::size_t n = qpcu::numel(p.shape);
+    for (std::size_t s = 0; s < runs.size(); ++s) {
+      if (objects) std::memcpy(objects + 2 * s * n, runs[s].object.data(), n * sizeof(qpcu::Complex));
+      if (supports) std::memcpy(supports + s * n, runs[s].support.data(), n);
+      if (errors) {
+        std::memcpy(errors + s * runs[s].errors.size(), runs[s].errors.data(),
+                    runs[s].errors.size() * sizeof(float));
+      }
+    }
+    *best = static_cast<int>(qpcu::best_index(runs));
+  });
+}
+
+// qpcu::cuda_available (solver.hpp:85) of the library's build.
+int qref_cuda_available(void) { return qpcu::cuda_available() ? 1 : 0; }
+
 int qref_run(void* solver, const void* ops, size_t count) {
   return guarded([&] {
     static_cast<RefSolver*>(solver)->solver->run(recipe_of(static_cast<const Op*>(ops), count));

@@ -29,7 +29,7 @@ LIBRARY = Path(__file__).resolve().parent / "libqpb.so"
 OK, INVALID_ARGUMENT, RUNTIME_ERROR, TIMEOUT = 0, 1, 2, 3
 
 AMP_STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
-VARIANTS = {"batched": 0, "plain": 1}
+VARIANTS = {"batched": 0, "plain": 1, "half": 2, "mixed": 3}
 SCHEDULES = {"auto": 0, "streamed": 1, "resident": 2}
 OP_KINDS = {"er": 0, "hio": 1, "raar": 2, "shrinkwrap": 3, "detwin_begin": 4, "detwin_end": 5}
 METHODS = {"max": 0, "rms": 1}
@@ -50,6 +50,7 @@ EXPORTS = (
     "qpb_results_device",
     "qpb_reset",
     "qpb_run",
+    "qpb_set_wait_limit",
     "qpb_set_progress",
     "qpb_error_count",
     "qpb_starts",
@@ -150,6 +151,7 @@ def load():
         lib.qpb_run.argtypes = [c_void_p, POINTER(Op), c_size_t]
         lib.qpb_reset.argtypes = [c_void_p, POINTER(Problem), c_size_t, c_uint64, c_void_p]
         lib.qpb_set_progress.argtypes = [c_void_p, PROGRESS, c_void_p]
+        lib.qpb_set_wait_limit.argtypes = [c_void_p, c_int, c_int]
         lib.qpb_error_count.argtypes = [c_void_p, POINTER(c_size_t)]
         lib.qpb_starts.argtypes = [c_void_p, POINTER(c_int)]
         lib.qpb_results.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]

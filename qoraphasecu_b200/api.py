@@ -348,7 +348,8 @@ def _ops(recipe):
 def _options(starts, batch, seed, start, sync_every, variant, amp_storage, device, stream,
              schedule):
     if variant not in _lib.VARIANTS:
-        raise ValueError(f"unknown variant '{variant}' (this backend has 'batched' and 'plain')")
+        raise ValueError(f"unknown variant '{variant}' (this backend has 'batched', 'plain', "
+                         "'half' and 'mixed')")
     if schedule not in _lib.SCHEDULES:
         raise ValueError(f"unknown schedule '{schedule}' (auto, streamed or resident)")
     if amp_storage not in _lib.AMP_STORAGE:
@@ -374,7 +375,7 @@ class Solver:
 
     def __init__(self, problem: Problem, *, starts: int = 1, batch: int | None = None,
                  seed: int | None = None, init=None, sync_every: int = 10,
-                 variant: Literal["batched", "plain"] = "batched",
+                 variant: Literal["batched", "plain", "half", "mixed"] = "batched",
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
                  device: int = -1, stream: int | None = None,
                  schedule: Literal["auto", "streamed", "resident"] = "auto"):
@@ -437,6 +438,13 @@ class Solver:
         _lib.check(self._lib.qpb_reset(self._handle, ctypes.byref(problem._c()), 1,
                                        0 if seed is None else seed, ptr))
         self.problem = problem
+
+    def set_wait_limit(self, polls: int, starve: bool = False):
+        """Polls a line pass's wait for its staged inputs makes before it gives
+        up (``run`` then raises TimeoutError); ``starve`` leaves the staged
+        copies out so that every such wait runs out, the fault injection of the
+        timeout tests (results are invalid until ``reset``)."""
+        _lib.check(self._lib.qpb_set_wait_limit(self._handle, int(polls), int(bool(starve))))
 
     def profile_passes(self, iterations: int = 20):
         """Mean device time (ms) of each line pass of one iteration, timed with
@@ -515,7 +523,7 @@ class BatchSolver:
 
     def __init__(self, problems, *, starts: int = 1, batch: int | None = None,
                  seed: int | None = None, init=None, sync_every: int = 10,
-                 variant: Literal["batched", "plain"] = "batched",
+                 variant: Literal["batched", "plain", "half", "mixed"] = "batched",
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
                  device: int = -1, stream: int | None = None,
                  schedule: Literal["auto", "streamed", "resident"] = "auto"):
@@ -689,7 +697,7 @@ def reconstruct(
     init=None,
     support_threshold: float = 0.1,
     backend: Literal["auto", "b200"] = "auto",
-    variant: Literal["batched", "plain"] = "batched",
+    variant: Literal["batched", "plain", "half", "mixed"] = "batched",
     sync_every: int = 10,
     amp_storage: Literal["f32", "f16", "bf16"] = "f32",
     progress=None,
@@ -712,8 +720,11 @@ def reconstruct(
             ``(starts, *shape)``, cut to the support.
         backend: ``"auto"`` or ``"b200"``; both run this backend, which needs
             a CUDA device.
-        variant: ``"batched"`` (graph-captured, all starts per launch) or
-            ``"plain"`` (one start per launch).
+        variant: ``"batched"`` (graph-captured, all starts per launch),
+            ``"plain"`` (one start per launch), or the fp16-storage forms of
+            batched: ``"half"`` (iterate and wave as fp16 pairs) and
+            ``"mixed"`` (fp16 wave for HIO and RAAR, FP32 iterate and ER);
+            both need power-of-two extents of 16..1024.
         amp_storage: ``"f32"``, ``"f16"`` or ``"bf16"`` storage of the amplitude.
         progress: ``fn(iteration, errors)`` every ``sync_every`` iterations.
         schedule: how batched iterations run: ``"streamed"`` line passes,

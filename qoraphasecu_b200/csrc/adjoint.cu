@@ -8,6 +8,7 @@
 // forward transform, the gradient's point-wise step with the loss sum on the
 // outer axis, inverse transform.
 
+#include <cstdint>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -39,11 +40,36 @@ AdjointResources& resources() {
   return *slot;
 }
 
+// Every loss becomes NaN when a line pass of this call gave up a bounded wait
+// (its CTAs wrote nothing, so the gradient is not valid); the counter is
+// cleared for the next call.
+__global__ void flag_failures_kernel(int* failures, double* loss, int batch) {
+  const bool failed = *failures != 0;
+  __syncthreads();
+  if (failed) {
+    for (int b = threadIdx.x; b < batch; b += blockDim.x) loss[b] = __longlong_as_double(0x7ff8000000000000LL);
+    if (threadIdx.x == 0) *failures = 0;
+  }
+}
+
+void require_aligned(const void* ptr, std::uintptr_t bytes, const char* name) {
+  if (reinterpret_cast<std::uintptr_t>(ptr) % bytes != 0) {
+    throw InvalidArgument(std::string("qpb_amplitude_loss_grad: ") + name + " must be " +
+                          std::to_string(bytes) + "-byte aligned");
+  }
+}
+
 }  // namespace
 
 void amplitude_loss_grad(int ndim, const long long* shape, int batch, const float* signed_amp,
                          const float2* x, float2* grad, double* loss, cudaStream_t stream) {
   if (batch < 1) throw InvalidArgument("batch must be >= 1");
+  // x, grad and the amplitude are moved by bulk copies, which start on
+  // 16-byte boundaries.
+  require_aligned(x, 16, "x");
+  require_aligned(grad, 16, "grad");
+  require_aligned(signed_amp, 16, "signed_amplitude");
+  require_aligned(loss, alignof(double), "loss");
   ProblemView view;
   view.ndim = ndim;
   for (int a = 0; a < ndim && a < 3; ++a) view.shape[a] = shape[a];
@@ -69,6 +95,9 @@ void amplitude_loss_grad(int ndim, const long long* shape, int batch, const floa
   runner.launch(Mode::kGrad, outer, params(Mode::kGrad, outer), stream);
   if (runner.has_mid()) runner.launch(Mode::kInv, 1, params(Mode::kInv, 1), stream);
   runner.launch(Mode::kInv, 2, params(Mode::kInv, 2), stream);
+  flag_failures_kernel<<<1, 32, 0, stream>>>(r.plans.wait_failures(), loss, batch);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
 }
 
 }  // namespace qpb

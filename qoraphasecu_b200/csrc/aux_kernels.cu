@@ -1,3 +1,5 @@
+#include <cuda_fp16.h>
+
 #include <algorithm>
 
 #include <stdexcept>
@@ -136,6 +138,14 @@ __global__ void scale_complex_kernel(float2* x, long long count, float scale) {
   QPB_FOR(i, count) { x[i] = cscale(x[i], scale); }
 }
 
+__global__ void to_half_kernel(const float2* in, __half2* out, long long count) {
+  QPB_FOR(i, count) { out[i] = __float22half2_rn(in[i]); }
+}
+
+__global__ void from_half_kernel(const __half2* in, float2* out, long long count) {
+  QPB_FOR(i, count) { out[i] = __half22float2(in[i]); }
+}
+
 // Occupies the stream for about `ns` nanoseconds of the device's global
 // timer, sleeping between reads; at most 4096 sleeps of 1 us, so it ends.
 __global__ void hold_stream_kernel(long long ns) {
@@ -225,6 +235,19 @@ void set_ctrl(Ctrl* ctrl, const Ctrl& value, cudaStream_t stream) {
 
 void scale_complex(float2* x, long long count, float scale, cudaStream_t stream) {
   scale_complex_kernel<<<grid(count, 1), kThreads, 0, stream>>>(x, count, scale);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+void to_half(const float2* in, void* out, long long count, cudaStream_t stream) {
+  to_half_kernel<<<grid(count, 1), kThreads, 0, stream>>>(in, static_cast<__half2*>(out), count);
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
+void from_half(const void* in, float2* out, long long count, cudaStream_t stream) {
+  from_half_kernel<<<grid(count, 1), kThreads, 0, stream>>>(static_cast<const __half2*>(in), out,
+                                                             count);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }

@@ -47,8 +47,13 @@ void set_coefficients(Ctrl* ctrl, float a, float b, cudaStream_t stream);
 // buffer has to outlive the call).
 void set_ctrl(Ctrl* ctrl, const Ctrl& value, cudaStream_t stream);
 
-// x[b][i] = x[b][i] / scale (complex), used for results of scaled storage.
+// x[i] = x[i] * scale (complex), used for results of scaled storage.
 void scale_complex(float2* x, long long count, float scale, cudaStream_t stream);
+
+// Complex64 <-> fp16 pairs (round to nearest; widening is exact), `count`
+// elements, for the fp16 iterate of the half variant.
+void to_half(const float2* in, void* out, long long count, cudaStream_t stream);
+void from_half(const void* in, float2* out, long long count, cudaStream_t stream);
 
 // Keeps `stream` busy for about `ns` nanoseconds (at most about 4 ms), so that
 // the host can queue timed work behind it and the device then runs that work

@@ -15,7 +15,7 @@ BatchSolver::BatchSolver(const std::vector<ProblemView>& problems, const SolverO
       stream_(options.stream),
       spp_(options.starts),
       every_(options.sync_every),
-      batched_(options.variant == Variant::kBatched),
+      batched_(options.variant != Variant::kPlain),
       on_device_(!problems.empty() && problems[0].on_device) {
   if (problems.empty()) throw InvalidArgument("no problems");
   if (options.starts < 1) throw InvalidArgument("starts must be >= 1");
@@ -124,7 +124,9 @@ void BatchSolver::run(const OpDesc* ops, std::size_t count) {
     for (int done = 0; done < o.n;) {
       const int len = classes_[0].solver->chunk_length(o.n - done);
       if (batched_) {
-        auto it = graphs_.find(len);
+        // graphs by chunk length and wave storage (the mixed variant switches it)
+        const int key = 2 * len + (classes_[0].solver->wave_half() ? 1 : 0);
+        auto it = graphs_.find(key);
         if (it == graphs_.end()) {
           for (Class& c : classes_) c.solver->prepare_branches();
           const unsigned long long before = launches();
@@ -148,7 +150,7 @@ void BatchSolver::run(const OpDesc* ops, std::size_t count) {
           QPB_CHECK(cudaStreamEndCapture(stream_, &graph));
           const unsigned long long kernels = launches() - before;
           count_launches(0ULL - kernels);  // counted again on every replay
-          it = graphs_.emplace(len, std::make_unique<Graph>(graph, kernels)).first;
+          it = graphs_.emplace(key, std::make_unique<Graph>(graph, kernels)).first;
         }
         it->second->launch(stream_);
       } else {
@@ -161,6 +163,12 @@ void BatchSolver::run(const OpDesc* ops, std::size_t count) {
     }
   }
   for (Class& c : classes_) c.solver->end_run();
+}
+
+void BatchSolver::set_wait(int tries, bool starve) {
+  stream_.sync();
+  graphs_.clear();
+  for (Class& c : classes_) c.solver->set_wait(tries, starve);
 }
 
 void BatchSolver::results(float2* objects, std::uint8_t* supports, float* errors) {

@@ -46,6 +46,9 @@ class BatchSolver {
   void set_progress(ProgressFn fn, void* user);
   // One shape class only (the per-pass profile of its solver).
   int profile_passes(int iterations, double* ms);
+  // Solver::set_wait for every shape class; the batch's own captured graphs
+  // are dropped too.
+  void set_wait(int tries, bool starve);
 
  private:
   struct Class {

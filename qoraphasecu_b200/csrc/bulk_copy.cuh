@@ -2,8 +2,9 @@
 // (sm_90+ cp.async.bulk), with a bounded wait.
 //
 // Every copy must start and end on 16-byte boundaries (addresses and size).
-// A wait gives up after kMaxWaitTries polls and returns false, so the caller
-// can record the failure; nothing here spins without limit.
+// A wait gives up after a bounded number of polls (kMaxWaitTries unless the
+// caller passes fewer) and returns false, so the caller can record the
+// failure; nothing here spins without limit.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -81,10 +82,11 @@ __device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, unsigned parit
   return done != 0;
 }
 
-// Waits for phase `parity` of `bar` to complete; false after kMaxWaitTries
+// Waits for phase `parity` of `bar` to complete; false after `tries`
 // unsuccessful polls.
-__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < kMaxWaitTries; ++i) {
+__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, unsigned parity,
+                                          int tries = kMaxWaitTries) {
+  for (int i = 0; i < tries; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
   }
   return false;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -80,6 +81,14 @@ qpb::AmpStorage storage_of(int s) {
 // The runtime's current device is per host thread: make the solver's current.
 void use_solver_device(const qpb_solver* solver) {
   QPB_CHECK(cudaSetDevice(solver->impl.device()));
+}
+
+// Device arrays a caller lends must be aligned to their element type.
+void require_aligned(const void* ptr, std::size_t bytes, const char* name) {
+  if (reinterpret_cast<std::uintptr_t>(ptr) % bytes != 0) {
+    throw qpb::InvalidArgument(std::string(name) + " must be " + std::to_string(bytes) +
+                               "-byte aligned");
+  }
 }
 
 }  // namespace
@@ -187,7 +196,7 @@ qpb::SolverOptions options_of(const qpb_options* options) {
   if (options->batch < 0 || (options->batch > 0 && options->starts % options->batch != 0)) {
     throw qpb::InvalidArgument("batch must divide starts");
   }
-  if (options->variant != QPB_VARIANT_BATCHED && options->variant != QPB_VARIANT_PLAIN) {
+  if (options->variant < QPB_VARIANT_BATCHED || options->variant > QPB_VARIANT_MIXED) {
     throw qpb::InvalidArgument("unknown variant");
   }
   if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_RESIDENT) {
@@ -240,6 +249,8 @@ qpb_status qpb_create_device(const qpb_problem* problem, const qpb_options* opti
     const qpb::SolverOptions o = options_of(options);
     qpb::ProblemView v = made_problem(problem);
     v.on_device = true;
+    require_aligned(v.amplitude, alignof(float), "amplitude");
+    require_aligned(o.start, alignof(float2), "options->start");
     if (!qpb_cuda_available()) throw std::runtime_error("no CUDA device available");
     *out = new qpb_solver({v}, o);
   });
@@ -261,6 +272,7 @@ qpb_status qpb_results_device(qpb_solver* solver, float* objects, uint8_t* suppo
                               float* errors) {
   return guarded([&] {
     require(solver != nullptr, "solver is NULL");
+    require_aligned(objects, alignof(float2), "objects");
     use_solver_device(solver);
     solver->impl.results_device(reinterpret_cast<float2*>(objects), supports, errors);
   });
@@ -331,6 +343,15 @@ qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out
     require(solver && ms_out && n_passes, "NULL argument");
     use_solver_device(solver);
     *n_passes = solver->impl.profile_passes(iterations, ms_out);
+  });
+}
+
+qpb_status qpb_set_wait_limit(qpb_solver* solver, int polls, int starve) {
+  return guarded([&] {
+    require(solver != nullptr, "solver is NULL");
+    require(polls >= 1, "polls must be >= 1");
+    use_solver_device(solver);
+    solver->impl.set_wait(polls, starve != 0);
   });
 }
 

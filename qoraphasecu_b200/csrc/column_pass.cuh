@@ -1,0 +1,27 @@
+// Column line passes whose tiles move by TMA tensor copies (column_pass.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "line_pass.cuh"
+
+namespace qpb {
+
+// False when the environment sets QPB_COLUMN_PASSES=0 (column passes then run
+// the register-resident kernels of fast_pass.cu; used to compare the two).
+bool column_passes_enabled();
+
+// Lines per CTA of the TMA column pass for `mode` with these parameters, or 0
+// when it does not take the pass: strided lines (S > 1) of 64, 128 or 256
+// points, CTAs of 8 adjacent columns that never span two starts, modes kMod
+// (p.amp_tiled == kAmpTiledLines: the amplitude tiled line-major in this
+// pass's CTA order), kFwd and kInv.
+int column_pass_lines(const PassParams& p, Mode mode);
+
+void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream);
+
+// Raises the dynamic shared-memory limit where needed; once per device,
+// outside stream capture.
+void configure_column_passes();
+
+}  // namespace qpb

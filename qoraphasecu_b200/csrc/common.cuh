@@ -77,6 +77,10 @@ struct Timeout : std::runtime_error {
 
 inline void cuda_check(cudaError_t status, const char* what) {
   if (status != cudaSuccess) {
+    // A non-sticky failure (an allocation, an invalid argument) stays the
+    // thread's last error; clear it so that a later launch check on this
+    // thread does not report it again.
+    (void)cudaGetLastError();
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(status));
   }
 }

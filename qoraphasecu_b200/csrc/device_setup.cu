@@ -80,9 +80,12 @@ __global__ void threshold_kernel(const float* mag, long long n, const unsigned* 
 }
 
 // Element e (FFT order) of one problem goes to index `tiled(e)` of the
-// signed-amplitude array: the modulus pass's CTA order for columns (element j
-// of line c of CTA tile t at (t * L + j) * lines + c), FFT order otherwise.
-__device__ __forceinline__ long long tiled_index(long long e, int L, int S, int lines) {
+// signed-amplitude array: the modulus pass's CTA order for columns, element j
+// of line c of CTA tile t at (t * L + j) * lines + c (element-major, the
+// register-resident pass) or at (t * lines + c) * L + j (line-major, the TMA
+// column pass); FFT order otherwise.
+__device__ __forceinline__ long long tiled_index(long long e, int L, int S, int lines,
+                                                 bool line_major) {
   if (lines <= 0 || S == 1) return e;
   const long long slab = static_cast<long long>(L) * S;
   const long long outer = e / slab;
@@ -90,7 +93,7 @@ __device__ __forceinline__ long long tiled_index(long long e, int L, int S, int 
   const long long j = rem / S;
   const long long col = rem - j * S;
   const long long tile = outer * (S / lines) + col / lines;
-  return (tile * L + j) * lines + col % lines;
+  return line_major ? (tile * lines + col % lines) * L + j : (tile * L + j) * lines + col % lines;
 }
 
 template <class T>
@@ -106,8 +109,10 @@ __device__ __forceinline__ __nv_bfloat16 from_float<__nv_bfloat16>(float v) {
 
 template <class T>
 __global__ void signed_kernel(const float* amp, const std::uint8_t* mask, long long n, int L, int S,
-                              int lines, T* out) {
-  QPB_LOOP(e, n) out[tiled_index(e, L, S, lines)] = from_float<T>(mask[e] ? -1.0f : amp[e]);
+                              int lines, bool line_major, T* out) {
+  QPB_LOOP(e, n) {
+    out[tiled_index(e, L, S, lines, line_major)] = from_float<T>(mask[e] ? -1.0f : amp[e]);
+  }
 }
 
 __global__ void nonzero_kernel(std::uint8_t* v, long long n) {
@@ -133,6 +138,30 @@ __global__ void __launch_bounds__(kEnergyThreads)
     for (int w = 0; w < kEnergyThreads / 32; ++w) t += partial[w];
     *out = t;
   }
+}
+
+// The amplitude's peak (one block; max of non-negative floats by their bits),
+// then amp /= peak, for fp16 storage of the wave: with the peak amplitude at 1
+// the stored transforms stay within fp16 range (the reference's
+// src/cuda/cuda_solver.cu:74-86). A zero amplitude keeps scale 1.
+__global__ void __launch_bounds__(kEnergyThreads)
+    peak_kernel(const float* amp, long long n, float* peak) {
+  __shared__ float partial[kEnergyThreads / 32];
+  float m = 0.0f;
+  for (long long i = threadIdx.x; i < n; i += kEnergyThreads) m = fmaxf(m, amp[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < kEnergyThreads / 32; ++w) t = fmaxf(t, partial[w]);
+    *peak = t > 0.0f ? t : 1.0f;
+  }
+}
+
+__global__ void normalise_kernel(float* amp, long long n, const float* peak) {
+  const float p = *peak;
+  QPB_LOOP(i, n) amp[i] = amp[i] / p;
 }
 
 constexpr std::size_t align256(std::size_t bytes) { return (bytes + 255) / 256 * 256; }
@@ -226,7 +255,7 @@ void make_problem_device(const float* intensity, int ndim, const long long* shap
   unsigned long long host_flags[2];
   QPB_CHECK(cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, stream));
   QPB_CHECK(cudaStreamSynchronize(stream));
-  check_waits();
+  check_waits(operator_plans(), stream);
   if (host_flags[0]) throw InvalidArgument("intensity contains NaN or Inf");
   if (mask && host_flags[1] == static_cast<unsigned long long>(n)) {
     throw InvalidArgument("mask marks every pixel as bad; nothing left to fit");
@@ -254,17 +283,25 @@ void autocorrelation_support_host(const float* intensity, int ndim, const long l
   support_device(dev_in, d, ndim, threshold, dev_out, scratch + in_bytes + align256(n), s);
   QPB_CHECK(cudaMemcpyAsync(out, dev_out, n, cudaMemcpyDeviceToHost, s));
   QPB_CHECK(cudaStreamSynchronize(s));
-  check_waits();
+  check_waits(operator_plans(), s);
 }
 
 std::size_t prepare_scratch_bytes(long long n) { return align256(static_cast<std::size_t>(n)); }
 
 void prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
-                            int lines, float* amp_fft, void* signed_out, std::uint8_t* support_fft,
-                            void* scratch, double* energy, cudaStream_t stream) {
+                            int lines, bool line_major, float* amp_fft, void* signed_out,
+                            std::uint8_t* support_fft, void* scratch, double* energy,
+                            float* peak, cudaStream_t stream) {
   const long long n = d.n();
   std::uint8_t* mask_fft = static_cast<std::uint8_t*>(scratch);
   roll<float>(q.amplitude, amp_fft, d, 1, true, stream);
+  if (peak) {
+    peak_kernel<<<1, kEnergyThreads, 0, stream>>>(amp_fft, n, peak);
+    QPB_CHECK(cudaGetLastError());
+    normalise_kernel<<<blocks_for(n), kThreads, 0, stream>>>(amp_fft, n, peak);
+    QPB_CHECK(cudaGetLastError());
+    count_launches(2);
+  }
   if (q.mask) {
     roll<std::uint8_t>(q.mask, mask_fft, d, 1, true, stream);
   } else {
@@ -276,15 +313,15 @@ void prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, i
   switch (storage) {
     case AmpStorage::kF32:
       signed_kernel<float><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft, n, L, S, lines, static_cast<float*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, line_major, static_cast<float*>(signed_out));
       break;
     case AmpStorage::kF16:
       signed_kernel<__half><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft, n, L, S, lines, static_cast<__half*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, line_major, static_cast<__half*>(signed_out));
       break;
     case AmpStorage::kBF16:
       signed_kernel<__nv_bfloat16><<<blocks_for(n), kThreads, 0, stream>>>(
-          amp_fft, mask_fft, n, L, S, lines, static_cast<__nv_bfloat16*>(signed_out));
+          amp_fft, mask_fft, n, L, S, lines, line_major, static_cast<__nv_bfloat16*>(signed_out));
       break;
   }
   QPB_CHECK(cudaGetLastError());

@@ -37,13 +37,17 @@ std::size_t prepare_scratch_bytes(long long n);
 
 // One problem's solver inputs from its device arrays (centre-origin): the FFT-
 // order FP32 amplitude, the signed amplitude (-1 masked) in `storage` written
-// to `signed_out` in the modulus pass's CTA order when `lines` > 0 and S > 1,
+// to `signed_out` in the modulus pass's CTA order when `lines` > 0 and S > 1
+// (tiles of `lines` lines, line-major inside a tile when `line_major`),
 // the FFT-order 0/1 support, and the usable energy (sum of A^2 over unmasked
 // pixels, in one fixed order: the same bits on every call) into the device
-// double `energy`. Enqueued on `stream`, which it does not synchronise.
-// `scratch`: prepare_scratch_bytes(n) device bytes, in use until the work ends.
+// double `energy`. With `peak` (a device float) the amplitude is first
+// divided by its peak, which `peak` receives (fp16 wave storage). Enqueued on
+// `stream`, which it does not synchronise. `scratch`:
+// prepare_scratch_bytes(n) device bytes, in use until the work ends.
 void prepare_problem_device(const ProblemView& q, Dims3 d, AmpStorage storage, int L, int S,
-                            int lines, float* amp_fft, void* signed_out, std::uint8_t* support_fft,
-                            void* scratch, double* energy, cudaStream_t stream);
+                            int lines, bool line_major, float* amp_fft, void* signed_out,
+                            std::uint8_t* support_fft, void* scratch, double* energy,
+                            float* peak, cudaStream_t stream);
 
 }  // namespace qpb

@@ -21,13 +21,11 @@
 #include "line_fft.cuh"
 #include "projection.cuh"
 #include "reduce.cuh"
+#include "storage.cuh"
 
 namespace qpb {
 
 namespace {
-
-// Bounded waits that gave up (read and cleared by take_fast_wait_failures).
-__device__ int g_fast_wait_failures = 0;
 
 __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 * 16; }
 
@@ -64,31 +62,37 @@ struct Tiling {
   static constexpr int SMEM = G::STAGES > 1 ? LINES * G::PITCH * 8 : 0;
 };
 
-template <int L, bool ROWS, Mode M, class AmpT>
+// WT, XT: storage of the wave and of the iterate (float2 or __half2).
+template <int L, bool ROWS, Mode M, class AmpT, class WT, class XT>
 struct Staging {
   using G = Tiling<L, ROWS>;
-  static constexpr int kTile = G::LINES * L * 8;  // one complex64 tile
+  using InT = std::conditional_t<M == Mode::kFwdFromX, XT, WT>;
+  static constexpr int kTileIn = G::LINES * L * static_cast<int>(sizeof(InT));
+  static constexpr int kTileOut = G::LINES * L * static_cast<int>(sizeof(WT));
+  static constexpr int kTile = kTileIn > kTileOut ? kTileIn : kTileOut;
   static constexpr bool kRowTma =
       ROWS && (M == Mode::kFwd || M == Mode::kFwdFromX || M == Mode::kInv || M == Mode::kUpd);
   static constexpr bool kAmp = M == Mode::kMod || M == Mode::kGrad;
   static constexpr bool kUpd = M == Mode::kUpd && ROWS;
   static constexpr int kExchange = align16(kRowTma && kTile > G::SMEM ? kTile : G::SMEM);
-  static constexpr int kSideA =
-      kAmp ? G::LINES * L * static_cast<int>(sizeof(AmpT)) : (kUpd ? kTile : 0);
+  static constexpr int kSideA = kAmp   ? G::LINES * L * static_cast<int>(sizeof(AmpT))
+                                : kUpd ? G::LINES * L * static_cast<int>(sizeof(XT))
+                                       : 0;
   static constexpr int kSideB = kUpd ? G::LINES * L : 0;
   static constexpr bool kBarrierUsed = kAmp || kUpd || kRowTma;
   static constexpr int kBarrier = align16(kExchange + kSideA + kSideB);
   static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : G::SMEM;
-  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTile % 16 == 0,
+  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTileIn % 16 == 0 && kTileOut % 16 == 0,
                 "bulk copies need 16-byte sizes");
 };
 
-template <int L, bool ROWS, Mode M, class AmpT>
+template <int L, bool ROWS, Mode M, class AmpT, class WT, class XT>
 __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS)
     fast_pass_kernel(const PassParams p) {
   using G = Geometry<L>;
   using Ti = Tiling<L, ROWS>;
-  using St = Staging<L, ROWS, M, AmpT>;
+  using St = Staging<L, ROWS, M, AmpT, WT, XT>;
+  using InT = typename St::InT;
   constexpr int E = G::E;
   constexpr int T = G::T;
   extern __shared__ float2 smem[];
@@ -113,8 +117,9 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     base = outer * static_cast<long long>(L) * p.S + inner + static_cast<long long>(t) * p.S;
     step = T * p.S;
   }
-  float2* __restrict__ wl = p.w + base;
-  float2* __restrict__ xl = p.x + base;
+  // Not __restrict__: an operator may transform an array in place (w == x).
+  WT* wl = reinterpret_cast<WT*>(p.w) + base;
+  XT* xl = reinterpret_cast<XT*>(p.x) + base;
   const float2* __restrict__ tw = p.stage_twiddle;
   // A row's T threads share a warp, so its exchanges need warp barriers only.
   constexpr bool kWarpLocal = ROWS && T <= 32;
@@ -145,7 +150,9 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   // amplitude tile of a modulus pass, the old iterate and support of a row
   // update. They hold no registers while in flight.
   unsigned char* sbase = reinterpret_cast<unsigned char*>(smem);
-  [[maybe_unused]] float2* wtile = smem;  // region W, rows of length L (bulk-copied passes)
+  // region W, rows of length L (bulk-copied passes): the input tile, later the output tile
+  [[maybe_unused]] const InT* in_tile = reinterpret_cast<const InT*>(smem);
+  [[maybe_unused]] WT* out_tile = reinterpret_cast<WT*>(smem);
   // Two barriers: `bar` for the input tile (or the amplitude), `side_bar` for
   // the old iterate and support of a row update, which are needed only after
   // the inverse transform, so their copies overlap it.
@@ -155,30 +162,33 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     if (tid == 0) {
       mbar_init(bar, 1);
       if constexpr (St::kUpd) {
-        mbar_arrive_expect_tx(bar, St::kTile);
+        mbar_arrive_expect_tx(bar, St::kTileIn);
         mbar_init(side_bar, 1);
         mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSideB);
       } else {
-        mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTile : 0) + St::kSideA + St::kSideB);
+        mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTileIn : 0) + St::kSideA + St::kSideB);
       }
     }
     __syncthreads();
+    // p.starve (tests of the timeout path) leaves every copy out, so the
+    // waits below run out with nothing in flight.
     if constexpr (St::kRowTma) {
-      if (tid == 0) {
-        const float2* src = (M == Mode::kFwdFromX ? p.x : p.w) + line0 * L;
-        bulk_g2s(wtile, src, St::kTile, bar);
+      if (tid == 0 && !p.starve) {
+        const InT* src = reinterpret_cast<const InT*>(M == Mode::kFwdFromX ? p.x : p.w) + line0 * L;
+        bulk_g2s(smem, src, St::kTileIn, bar);
       }
     }
     if constexpr (St::kUpd) {
-      if (tid == 0) {
-        bulk_g2s(sbase + St::kExchange, p.x + line0 * L, St::kSideA, side_bar);
+      if (tid == 0 && !p.starve) {
+        bulk_g2s(sbase + St::kExchange, reinterpret_cast<const XT*>(p.x) + line0 * L, St::kSideA,
+                 side_bar);
         bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, side_bar);
       }
     } else if constexpr (St::kAmp) {
       if (ROWS || p.amp_tiled) {
         // FFT-order rows, or the amplitude pre-tiled in this pass's CTA order:
         // the CTA's tile is one contiguous block.
-        if (tid == 0) {
+        if (tid == 0 && !p.starve) {
           const long long line_in_start =
               line0 - static_cast<long long>(batch_start) * p.lines_per_start;
           const AmpT* src = static_cast<const AmpT*>(p.amp) +
@@ -191,7 +201,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
         const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
                           (outer * static_cast<long long>(L) * p.S + (line0 - outer * p.S) - start_off);
         constexpr int kRowBytes = Ti::LINES * static_cast<int>(sizeof(AmpT));
-        for (int j = tid; j < L; j += Ti::NT) {
+        for (int j = tid; j < L && !p.starve; j += Ti::NT) {
           bulk_g2s(sbase + St::kExchange + j * kRowBytes, src + static_cast<long long>(j) * p.S,
                    kRowBytes, bar);
         }
@@ -199,11 +209,18 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     }
   }
 
-  // Every thread waits (bounded); if any gave up, the CTA records it and
-  // leaves together, writing nothing.
+  // Every thread waits (bounded); if any gave up, the CTA leaves together,
+  // writing nothing. Before it leaves, thread 0 waits once more (bounded
+  // again) on every barrier whose copies may still be in flight, so that no
+  // copy lands in the shared memory of a CTA that has exited, and records the
+  // failure in the launching owner's counter.
   auto staged = [&](std::uint64_t* b) -> bool {
-    if (!__syncthreads_and(mbar_wait(b, 0) ? 1 : 0)) {
-      if (tid == 0) atomicAdd(&g_fast_wait_failures, 1);
+    if (!__syncthreads_and(mbar_wait(b, 0, p.wait_tries) ? 1 : 0)) {
+      if (tid == 0) {
+        mbar_wait(bar, 0, p.wait_tries);
+        if constexpr (St::kUpd) mbar_wait(side_bar, 0, p.wait_tries);
+        atomicAdd(p.wait_failures, 1);
+      }
       return false;
     }
     return true;
@@ -213,18 +230,18 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   if constexpr (St::kRowTma) {
     if (!staged(bar)) return;
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = wtile[l * L + t + T * m];
+    for (int m = 0; m < E; ++m) v[m] = load_c(in_tile[l * L + t + T * m]);
     __syncthreads();  // region W becomes the exchange buffer
   } else {
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       if constexpr (M == Mode::kFwdFromX) {
-        v[m] = xl[m * step];
+        v[m] = load_c(xl[m * step]);
       } else if constexpr (M == Mode::kBlurMag) {
-        const float2 xv = xl[m * step];
+        const float2 xv = load_c(xl[m * step]);
         v[m] = {sqrtf(xv.x * xv.x + xv.y * xv.y), 0.0f};
       } else {
-        v[m] = wl[m * step];
+        v[m] = load_c(wl[m * step]);
       }
     }
   }
@@ -249,7 +266,8 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     for (int m = 0; m < E; ++m) {
       const int j = t + T * m;
       const float a = to_float(ROWS ? amp_tile[l * L + j] : amp_tile[j * Ti::LINES + l]);
-      v[m] = pointwise_projection<M>(v[m], a, s, acc);
+      // an fp16 wave defers the inverse's 1/sqrt(n) to the update pass
+      v[m] = pointwise_projection<M>(v[m], a, s, acc, kHalfStorage<WT> ? 1.0f : s);
     }
     // one call per CTA; its first barrier also orders the forward transform's
     // exchange reads before the inverse's writes
@@ -260,35 +278,35 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     if constexpr (St::kUpd) {
       if (!staged(side_bar)) return;
       // x_new replaces the old iterate in its tile and leaves by one bulk store.
-      float2* x_tile = reinterpret_cast<float2*>(sbase + St::kExchange);
+      XT* x_tile = reinterpret_cast<XT*>(sbase + St::kExchange);
       const std::uint8_t* s_tile = sbase + St::kExchange + St::kSideA;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int j = l * L + t + T * m;
-        float2 xn = v[m];
+        float2 xn = kHalfStorage<WT> ? cscale(v[m], p.scale) : v[m];
         if (!s_tile[j]) {
-          const float2 xo = x_tile[j];
+          const float2 xo = load_c(x_tile[j]);
           xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
         }
-        x_tile[j] = xn;
+        x_tile[j] = store_c<XT>(xn);
         v[m] = xn;
       }
       fence_proxy_async();
       __syncthreads();
       if (tid == 0) {
-        bulk_s2g(p.x + line0 * L, x_tile, St::kTile);
+        bulk_s2g(reinterpret_cast<XT*>(p.x) + line0 * L, x_tile, St::kSideA);
         bulk_commit();
       }
     } else {
       const std::uint8_t* __restrict__ sl = p.support + base;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
-        float2 xn = v[m];
+        float2 xn = kHalfStorage<WT> ? cscale(v[m], p.scale) : v[m];
         if (!sl[m * step]) {
-          const float2 xo = xl[m * step];
+          const float2 xo = load_c(xl[m * step]);
           xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
         }
-        xl[m * step] = xn;
+        xl[m * step] = store_c<XT>(xn);
         v[m] = xn;
       }
       __syncthreads();
@@ -311,11 +329,11 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     // tile goes there and leaves by one bulk store.
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < E; ++m) wtile[l * L + t + T * m] = v[m];
+    for (int m = 0; m < E; ++m) out_tile[l * L + t + T * m] = store_c<WT>(v[m]);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      bulk_s2g(p.w + line0 * L, wtile, St::kTile);
+      bulk_s2g(reinterpret_cast<WT*>(p.w) + line0 * L, out_tile, St::kTileOut);
       bulk_commit();
       bulk_wait_reads();
     }
@@ -327,7 +345,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   unsigned cnt = 0;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    wl[m * step] = v[m];
+    wl[m * step] = store_c<WT>(v[m]);
     if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
       if (p.level_method == 1) {
         peak = fmaxf(peak, v[m].x);
@@ -353,29 +371,57 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   }
 }
 
-template <int L, bool ROWS, Mode M, class AmpT>
+template <int L, bool ROWS, Mode M, class AmpT, class WT, class XT>
 void launch_one(const PassParams& p, cudaStream_t stream) {
   using Ti = Tiling<L, ROWS>;
   const dim3 grid(static_cast<unsigned>(p.lines / Ti::LINES));
-  fast_pass_kernel<L, ROWS, M, AmpT>
-      <<<grid, Ti::NT, Staging<L, ROWS, M, AmpT>::kBytes, stream>>>(p);
+  fast_pass_kernel<L, ROWS, M, AmpT, WT, XT>
+      <<<grid, Ti::NT, Staging<L, ROWS, M, AmpT, WT, XT>::kBytes, stream>>>(p);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }
 
+// Storage combinations built: complex64 wave and iterate for every mode; an
+// fp16 wave with an fp16 or complex64 iterate for the modes of an iteration
+// and of the wave's set-up (FP32 amplitude); the blur of an fp16 iterate into
+// a complex64 wave (shrinkwrap). Modes that do not touch x use one kernel for
+// either iterate storage.
+template <Mode M>
+inline constexpr bool kHalfWaveMode = M == Mode::kFwd || M == Mode::kFwdFromX ||
+                                      M == Mode::kInv || M == Mode::kMod || M == Mode::kUpd;
+template <Mode M>
+inline constexpr bool kTouchesX = M == Mode::kFwdFromX || M == Mode::kUpd || M == Mode::kBlurMag;
+
 template <int L, bool ROWS, Mode M>
 void launch_storage(const PassParams& p, cudaStream_t stream) {
+  if (p.wave_half || (kTouchesX<M> && p.iter_half)) {
+    if (p.amp_storage != AmpStorage::kF32) {
+      throw std::logic_error("fast line pass: fp16 storage runs with an FP32 amplitude");
+    }
+    if constexpr (kHalfWaveMode<M>) {
+      if (p.wave_half) {
+        if (p.iter_half || !kTouchesX<M>) {
+          return launch_one<L, ROWS, M, float, __half2, __half2>(p, stream);
+        }
+        return launch_one<L, ROWS, M, float, __half2, float2>(p, stream);
+      }
+    }
+    if constexpr (M == Mode::kBlurMag) {
+      if (!p.wave_half) return launch_one<L, ROWS, M, float, float2, __half2>(p, stream);
+    }
+    throw std::logic_error("fast line pass: no kernel for this storage and mode");
+  }
   if constexpr (M == Mode::kMod || M == Mode::kGrad) {
     switch (p.amp_storage) {
       case AmpStorage::kF32:
-        return launch_one<L, ROWS, M, float>(p, stream);
+        return launch_one<L, ROWS, M, float, float2, float2>(p, stream);
       case AmpStorage::kF16:
-        return launch_one<L, ROWS, M, __half>(p, stream);
+        return launch_one<L, ROWS, M, __half, float2, float2>(p, stream);
       case AmpStorage::kBF16:
-        return launch_one<L, ROWS, M, __nv_bfloat16>(p, stream);
+        return launch_one<L, ROWS, M, __nv_bfloat16, float2, float2>(p, stream);
     }
   } else {
-    launch_one<L, ROWS, M, float>(p, stream);
+    launch_one<L, ROWS, M, float, float2, float2>(p, stream);
   }
 }
 
@@ -445,13 +491,19 @@ int fast_lines(int L, bool rows) {
   }
 }
 
-template <int L, bool ROWS, Mode M, class AmpT>
+template <int L, bool ROWS, Mode M, class AmpT, class WT = float2, class XT = float2>
 void allow_smem_one() {
-  constexpr int bytes = Staging<L, ROWS, M, AmpT>::kBytes;
+  constexpr int bytes = Staging<L, ROWS, M, AmpT, WT, XT>::kBytes;
   if constexpr (bytes > 48 * 1024) {
-    QPB_CHECK(cudaFuncSetAttribute(fast_pass_kernel<L, ROWS, M, AmpT>,
+    QPB_CHECK(cudaFuncSetAttribute(fast_pass_kernel<L, ROWS, M, AmpT, WT, XT>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   }
+}
+
+template <int L, bool ROWS, Mode M>
+void allow_smem_half() {
+  allow_smem_one<L, ROWS, M, float, __half2, __half2>();
+  if constexpr (kTouchesX<M>) allow_smem_one<L, ROWS, M, float, __half2, float2>();
 }
 
 template <int L, bool ROWS>
@@ -468,6 +520,12 @@ void allow_smem_modes() {
   allow_smem_one<L, ROWS, Mode::kGrad, float>();
   allow_smem_one<L, ROWS, Mode::kGrad, __half>();
   allow_smem_one<L, ROWS, Mode::kGrad, __nv_bfloat16>();
+  allow_smem_half<L, ROWS, Mode::kFwd>();
+  allow_smem_half<L, ROWS, Mode::kFwdFromX>();
+  allow_smem_half<L, ROWS, Mode::kInv>();
+  allow_smem_half<L, ROWS, Mode::kMod>();
+  allow_smem_half<L, ROWS, Mode::kUpd>();
+  allow_smem_one<L, ROWS, Mode::kBlurMag, float, float2, __half2>();
 }
 
 template <int L>
@@ -504,16 +562,6 @@ bool fast_passes_enabled() {
 
 int fast_pass_lines(const PassParams& p) {
   return fast_passes_enabled() && fast_pass_supports(p) ? fast_lines(p.L, p.S == 1) : 0;
-}
-
-int take_fast_wait_failures() {
-  int failures = 0;
-  QPB_CHECK(cudaMemcpyFromSymbol(&failures, g_fast_wait_failures, sizeof(int)));
-  if (failures) {
-    const int zero = 0;
-    QPB_CHECK(cudaMemcpyToSymbol(g_fast_wait_failures, &zero, sizeof(int)));
-  }
-  return failures;
 }
 
 bool fast_pass_supports(const PassParams& p) {

@@ -23,10 +23,6 @@ bool fast_passes_enabled();
 // Lines per CTA of the register-resident kernel for this pass (0: not used).
 int fast_pass_lines(const PassParams& p);
 
-// Number of CTAs whose bounded wait for their staged inputs gave up since the
-// last call (those CTAs wrote nothing); reading clears it. Synchronises.
-int take_fast_wait_failures();
-
 // Raises the dynamic shared-memory limit of the kernels that need more than
 // 48 KiB; once per device, outside stream capture.
 void configure_fast_passes();

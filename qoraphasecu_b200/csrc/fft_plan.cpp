@@ -49,6 +49,30 @@ PlanCache::~PlanCache() {
   for (void* p : allocations_) cudaFree(p);
 }
 
+int* PlanCache::wait_failures() {
+  std::lock_guard<std::mutex> lock(mutex_);
+  if (!failures_) {
+    void* dev = nullptr;
+    QPB_CHECK(cudaMalloc(&dev, sizeof(int)));
+    allocations_.push_back(dev);
+    QPB_CHECK(cudaMemset(dev, 0, sizeof(int)));
+    failures_ = static_cast<int*>(dev);
+  }
+  return failures_;
+}
+
+int PlanCache::take_wait_failures(cudaStream_t stream) {
+  int* counter = wait_failures();
+  int failures = 0;
+  QPB_CHECK(cudaMemcpyAsync(&failures, counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  QPB_CHECK(cudaStreamSynchronize(stream));
+  if (failures) {
+    QPB_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
+    QPB_CHECK(cudaStreamSynchronize(stream));
+  }
+  return failures;
+}
+
 const LinePlan& PlanCache::get(int length) {
   std::lock_guard<std::mutex> lock(mutex_);
   if (auto it = plans_.find(length); it != plans_.end()) return it->second;

@@ -43,10 +43,21 @@ class PlanCache {
 
   const LinePlan& get(int length);
 
+  // Device counter of the line-pass CTAs whose bounded wait for their staged
+  // inputs gave up (those CTAs wrote nothing), shared by every pass planned
+  // from this cache: a solver's own cache makes it per solver. Allocated and
+  // zeroed on first use, which must not fall inside a stream capture.
+  int* wait_failures();
+
+  // Reads the counter on `stream` after the work enqueued there, clears it
+  // when it is set, and returns what it held. Synchronises `stream`.
+  int take_wait_failures(cudaStream_t stream);
+
  private:
   std::mutex mutex_;
   std::map<int, LinePlan> plans_;
   std::vector<void*> allocations_;
+  int* failures_ = nullptr;
 };
 
 }  // namespace qpb

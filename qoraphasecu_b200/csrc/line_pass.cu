@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "butterfly.cuh"
+#include "column_pass.cuh"
 #include "fast_pass.cuh"
 #include "line_pass.cuh"
 #include "projection.cuh"
@@ -351,6 +352,7 @@ void configure_line_passes() {
   allow_smem(line_pass_kernel<Mode::kGrad, __half>);
   allow_smem(line_pass_kernel<Mode::kGrad, __nv_bfloat16>);
   configure_fast_passes();
+  configure_column_passes();
 }
 
 int choose_lpc(int L, int S, int lines_per_start) {
@@ -364,7 +366,15 @@ int choose_lpc(int L, int S, int lines_per_start) {
 }
 
 void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
+  if (column_pass_lines(p, mode) > 0) return launch_column_pass(mode, p, stream);
+  if (p.amp_tiled == kAmpTiledLines) {
+    throw std::logic_error("line pass: a line-major tiled amplitude needs the column pass");
+  }
   if (fast_passes_enabled() && fast_pass_supports(p)) return launch_fast_pass(mode, p, stream);
+  const bool touches_x = mode == Mode::kFwdFromX || mode == Mode::kUpd || mode == Mode::kBlurMag;
+  if (p.wave_half || (touches_x && p.iter_half)) {
+    throw std::logic_error("line pass: fp16 storage needs the register-resident or column pass");
+  }
   if (p.amp_tiled) throw std::logic_error("line pass: tiled amplitude needs the register-resident pass");
   if (p.lines % p.lpc != 0 || p.lines_per_start % p.lpc != 0) {
     throw std::logic_error("line pass: lines per CTA must divide the lines of a start");

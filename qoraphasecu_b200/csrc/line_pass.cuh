@@ -83,11 +83,30 @@ struct PassParams {
   int coef_from_ctrl;
   int bump_counter;               // kUpd increments ctrl->counters[group]
   AmpStorage amp_storage;
-  // The amplitude is stored in the CTA order of a register-resident modulus
-  // pass (written so by the problem set-up's signed_kernel) instead of FFT
-  // order: one contiguous tile per CTA.
+  // The amplitude is stored in the CTA order of the modulus pass (written so
+  // by the problem set-up's signed_kernel) instead of FFT order: one
+  // contiguous tile per CTA, element-major for the register-resident pass
+  // (kAmpTiledElements) or line-major for the TMA column pass
+  // (kAmpTiledLines); 0 = FFT order.
   int amp_tiled;
+  // Bounded waits of the staged (bulk-copied) inputs: polls before a wait
+  // gives up, and the device counter a CTA that gave up increments (owned by
+  // whoever launches the pass and checked by it afterwards).
+  int wait_tries;
+  int* wait_failures;
+  // Fault injection for the tests of the timeout path: the staged copies are
+  // not issued, so every staged wait runs out (nothing is left in flight).
+  int starve;
+  // Storage of the wave (w) and of the iterate (x): 0 complex64, 1 fp16
+  // pairs (__half2; x and w then point at half2 arrays). With an fp16 wave a
+  // modulus pass leaves the inverse's 1/sqrt(n) to the update pass, which
+  // applies it after its inverse transform (values stay in fp16 range).
+  int wave_half;
+  int iter_half;
 };
+
+inline constexpr int kAmpTiledElements = 1;
+inline constexpr int kAmpTiledLines = 2;
 
 // Element offset of the amplitude that global start `start` reads.
 QPB_HD long long amp_offset(const PassParams& p, int start) {

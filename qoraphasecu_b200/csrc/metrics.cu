@@ -268,7 +268,7 @@ void align(const float2* a, const float2* reference, int ndim, const long long* 
   QPB_CHECK(cudaMemcpyAsync(host.data(), acc.get(), host.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, s));
   s.sync();
-  check_waits();
+  check_waits(t.plans, s);
   std::vector<int> choice(static_cast<std::size_t>(batch));
   for (int b = 0; b < batch; ++b) {
     float e[2];
@@ -326,7 +326,7 @@ void simulate_intensity(const float2* object, int ndim, const long long* shape, 
   QPB_CHECK(cudaMemcpyAsync(out, centred.get(), static_cast<std::size_t>(n) * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
   s.sync();
-  check_waits();
+  check_waits(t.plans, s);
 }
 
 }  // namespace qpb

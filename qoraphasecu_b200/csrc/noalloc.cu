@@ -11,15 +11,19 @@
 //
 // Limits: at most kNoAllocMaxElements elements per array, at most
 // kNoAllocMaxLine along any axis. The array is shared by every call on a
-// device and keeps the last call's contents; calls that overlap on the GPU
-// race on it.
+// device and keeps the last call's contents (the twiddle tables of the last
+// shape are reused by a call of the same shape); calls that overlap on the
+// GPU race on it.
 
+#include <array>
 #include <cmath>
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <string>
 
 #include "../../include/qpb.h"
+#include "bulk_copy.cuh"
 #include "fft_plan.hpp"
 #include "line_pass.cuh"
 #include "reduce.cuh"
@@ -37,6 +41,7 @@ constexpr std::size_t kCtrlOffset = 0;       // Ctrl
 constexpr std::size_t kCounterOffset = 64;   // int
 constexpr std::size_t kErrOffset = 128;      // double: Fourier-error numerator
 constexpr std::size_t kEnergyOffset = 136;   // double: usable energy
+constexpr std::size_t kFailOffset = 144;     // int: line-pass CTAs whose bounded wait gave up
 constexpr std::size_t kTwiddleOffset = 256;  // 3 axes x kNoAllocMaxLine float2
 constexpr std::size_t kAmpOffset = kTwiddleOffset + 3 * kNoAllocMaxLine * sizeof(float2);
 constexpr std::size_t kScratchBytes = kAmpOffset + kNoAllocMaxElements * sizeof(float);
@@ -45,20 +50,36 @@ static_assert(kNoAllocMaxLine >= 2 * 1024, "an axis slot holds W_L^k and the sta
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of the scratch array, looked up once per device. In host
-// code `g_noalloc_scratch` is only a stand-in for the symbol, never an address.
-unsigned char* scratch_address() {
-  static std::mutex mutex;
-  static std::map<int, unsigned char*> addresses;
+// Per device: the scratch array's device address, looked up once (in host
+// code `g_noalloc_scratch` is only a stand-in for the symbol, never an
+// address), and the line length whose twiddle tables each axis slot holds, so
+// that a call of the shape before rebuilds none of them.
+struct ScratchState {
+  unsigned char* base = nullptr;
+  std::array<int, 3> table_length{0, 0, 0};
+};
+
+std::mutex g_scratch_mutex;
+
+ScratchState& scratch_state() {
+  static std::map<int, ScratchState> states;
   int device = 0;
   QPB_CHECK(cudaGetDevice(&device));
-  std::lock_guard<std::mutex> lock(mutex);
-  auto it = addresses.find(device);
-  if (it != addresses.end()) return it->second;
-  void* ptr = nullptr;
-  QPB_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-  configure_line_passes();
-  return addresses.emplace(device, static_cast<unsigned char*>(ptr)).first->second;
+  ScratchState& state = states[device];
+  if (!state.base) {
+    void* ptr = nullptr;
+    QPB_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    configure_line_passes();
+    state.base = static_cast<unsigned char*>(ptr);
+  }
+  return state;
+}
+
+void require_aligned(const void* ptr, std::uintptr_t bytes, const char* name) {
+  if (reinterpret_cast<std::uintptr_t>(ptr) % bytes != 0) {
+    throw InvalidArgument(std::string("qpb_modulus_project_noalloc: ") + name +
+                          " must be " + std::to_string(bytes) + "-byte aligned");
+  }
 }
 
 // Resets the control block and the accumulators a call starts from.
@@ -66,6 +87,7 @@ __global__ void reset_kernel(unsigned char* base) {
   auto* ctrl = reinterpret_cast<Ctrl*>(base + kCtrlOffset);
   auto* counter = reinterpret_cast<int*>(base + kCounterOffset);
   *counter = 0;
+  *reinterpret_cast<int*>(base + kFailOffset) = 0;
   *reinterpret_cast<double*>(base + kErrOffset) = 0.0;
   *reinterpret_cast<double*>(base + kEnergyOffset) = 0.0;
   ctrl->errs = reinterpret_cast<double*>(base + kErrOffset);
@@ -107,8 +129,12 @@ __global__ void signed_amplitude_kernel(const float* amp, const std::uint8_t* ma
   if (threadIdx.x == 0) atomicAdd(energy, e);
 }
 
-__global__ void finalize_kernel(const double* num, const double* energy, float* error_out) {
-  *error_out = static_cast<float>(sqrt(*num / (*energy + static_cast<double>(kEps))));
+// The Fourier error, or NaN when a line pass gave up a bounded wait (its CTAs
+// wrote nothing, so `out` is not the projection).
+__global__ void finalize_kernel(const double* num, const double* energy, const int* failures,
+                                float* error_out) {
+  *error_out = *failures ? __int_as_float(0x7fc00000)
+                         : static_cast<float>(sqrt(*num / (*energy + static_cast<double>(kEps))));
 }
 
 void check_launch() {
@@ -130,6 +156,11 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
     if (!shape || !amplitude || !x || !out || !error_out) {
       throw InvalidArgument("NULL argument");
     }
+    // x and out are moved by bulk copies, which start on 16-byte boundaries.
+    require_aligned(x, 16, "x");
+    require_aligned(out, 16, "out");
+    require_aligned(amplitude, alignof(float), "amplitude");
+    require_aligned(error_out, alignof(float), "error_out");
     if (ndim != 2 && ndim != 3) {
       throw InvalidArgument("shape must be 2D or 3D, got ndim=" + std::to_string(ndim));
     }
@@ -151,7 +182,9 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
                             std::to_string(kNoAllocMaxElements));
     }
     const auto s = static_cast<cudaStream_t>(stream);
-    unsigned char* base = scratch_address();
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    ScratchState& state = scratch_state();
+    unsigned char* base = state.base;
     auto* ctrl = reinterpret_cast<Ctrl*>(base + kCtrlOffset);
     auto* twiddles = reinterpret_cast<float2*>(base + kTwiddleOffset);
     auto* signed_amp = reinterpret_cast<float*>(base + kAmpOffset);
@@ -164,22 +197,24 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
       const int L = dims[a];
       const auto radices = factorize(L);
       float2* tw = twiddles + a * kNoAllocMaxLine;
-      twiddle_kernel<<<(L + 255) / 256, 256, 0, s>>>(tw, L);
-      check_launch();
+      const StageGeometry g = stage_geometry(L);
+      if (state.table_length[a] != L) {
+        twiddle_kernel<<<(L + 255) / 256, 256, 0, s>>>(tw, L);
+        check_launch();
+        if (g.count > 0) {
+          // after the L entries of W_L^k in the axis's slot (L + count <= 2 L)
+          stage_twiddle_kernel<<<(g.count + 255) / 256, 256, 0, s>>>(tw, tw + L, L, g);
+          check_launch();
+        }
+        state.table_length[a] = L;
+      }
       PassParams& p = axis_params[a];
       p.w = reinterpret_cast<float2*>(out);
       p.x = const_cast<float2*>(reinterpret_cast<const float2*>(x));
       p.amp = signed_amp;
       p.ctrl = ctrl;
       p.twiddle = tw;
-      p.stage_twiddle = tw;
-      const StageGeometry g = stage_geometry(L);
-      if (g.count > 0) {
-        // after the L entries of W_L^k in the axis's slot (L + count <= 2 L)
-        stage_twiddle_kernel<<<(g.count + 255) / 256, 256, 0, s>>>(tw, tw + L, L, g);
-        check_launch();
-        p.stage_twiddle = tw + L;
-      }
+      p.stage_twiddle = g.count > 0 ? tw + L : tw;
       p.n = n;
       p.L = L;
       p.S = a == 2 ? 1 : a == 1 ? dims[2] : dims[1] * dims[2];
@@ -191,6 +226,8 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
       p.scale = 1.0f / std::sqrt(static_cast<float>(n));
       p.starts_total = 1;
       p.amp_storage = AmpStorage::kF32;
+      p.wait_tries = kMaxWaitTries;
+      p.wait_failures = reinterpret_cast<int*>(base + kFailOffset);
     }
     signed_amplitude_kernel<<<static_cast<int>((n + 255) / 256), 256, 0, s>>>(
         amplitude, mask, signed_amp, n, reinterpret_cast<double*>(base + kEnergyOffset));
@@ -203,7 +240,7 @@ extern "C" qpb_status qpb_modulus_project_noalloc(int ndim, const int64_t* shape
     launch_line_pass(Mode::kInv, axis_params[2], s);
     finalize_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const double*>(base + kErrOffset),
                                     reinterpret_cast<const double*>(base + kEnergyOffset),
-                                    error_out);
+                                    reinterpret_cast<const int*>(base + kFailOffset), error_out);
     check_launch();
     return QPB_OK;
   } catch (const std::invalid_argument& e) {

@@ -32,23 +32,24 @@ __device__ __forceinline__ float to_float(AmpT a) {
 // 2 (y - P_M y) = 2 (1 - A / (|y| + eps)) y on usable pixels and 0 on masked
 // ones, whose inverse transform is the gradient of sum (|F x| - A)^2 in
 // PyTorch's convention (dL/dRe + i dL/dIm).
+//   `out_scale` multiplies the result (s unless the caller defers the inverse's
+// 1/sqrt(n) to after the inverse transform, as the fp16 wave storage does to
+// keep stored values in range: src/cuda/device.cuh:14-16 of the reference).
 template <Mode M>
-__device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float s, float& acc) {
+__device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float s, float& acc,
+                                                       float out_scale) {
   const float re = v.x * s;
   const float im = v.y * s;
-  const float ss = re * re + im * im;
-  // 1 / sqrt(|y|^2 + eps^2) stands for 1 / (|y| + eps): equal in FP32 unless
-  // |y| is within a few orders of magnitude of eps = 1e-12, and 0 -> 0 like the
-  // reference. rsqrtf is the hardware approximation (<= 2 ulp), branch-free.
-  const float rinv = rsqrtf(ss + kEps * kEps);
-  const float mag = ss * rinv;
+  // The reference's own expression, rounded the same way: an IEEE square root
+  // of the squared magnitude and an IEEE division by (|y| + eps).
+  const float mag = sqrtf(re * re + im * im);
   float f;
   if constexpr (M == Mode::kGrad) {
     f = 0.0f;
     if (a >= 0.0f) {
       const float d = mag - a;
       acc += d * d;
-      f = 2.0f * (1.0f - a * rinv) * s;
+      f = 2.0f * (1.0f - a / (mag + kEps)) * out_scale;
     }
   } else {
     float target = mag;
@@ -57,9 +58,14 @@ __device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float 
       acc += d * d;
       target = a;
     }
-    f = target * rinv * s;
+    f = target / (mag + kEps) * out_scale;
   }
   return {re * f, im * f};
+}
+
+template <Mode M>
+__device__ __forceinline__ float2 pointwise_projection(float2 v, float a, float s, float& acc) {
+  return pointwise_projection<M>(v, a, s, acc, s);
 }
 
 }  // namespace qpb

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include "bulk_copy.cuh"
+#include "column_pass.cuh"
 #include "device_setup.cuh"
 #include "fast_pass.cuh"
 #include "resident.cuh"
@@ -73,9 +75,8 @@ void trace(const char* fmt, ...) {
   va_end(args);
 }
 
-// Throws Timeout when a kernel's bounded wait gave up since the last check.
-void check_waits() {
-  if (const int failed = take_fast_wait_failures()) {
+void check_waits(PlanCache& plans, cudaStream_t stream) {
+  if (const int failed = plans.take_wait_failures(stream)) {
     throw Timeout(std::to_string(failed) +
                   " line-pass CTAs gave up waiting for their staged inputs; results are invalid");
   }
@@ -215,7 +216,8 @@ int recipe_iterations(const OpDesc* ops, std::size_t count) {
 }
 
 // ------------------------------------------------------------------ PassRunner
-PassRunner::PassRunner(Dims3 d, int ndim, PlanCache& plans) : d_(d), ndim_(ndim) {
+PassRunner::PassRunner(Dims3 d, int ndim, PlanCache& plans)
+    : d_(d), ndim_(ndim), wait_failures_(plans.wait_failures()), wait_tries_(kMaxWaitTries) {
   configure_line_passes();
   for (int a = 0; a < 3; ++a) {
     plans_[a] = (ndim == 2 && a == 0) ? nullptr : &plans.get(axis_len(d, a));
@@ -239,6 +241,9 @@ PassParams PassRunner::params(Mode mode, int axis3, int batch) const {
   p.scale = 1.0f / std::sqrt(static_cast<float>(p.n));
   p.amp_stride = 0;
   p.starts_per_problem = 1;
+  p.wait_tries = wait_tries_;
+  p.wait_failures = wait_failures_;
+  p.starve = starve_ ? 1 : 0;
   return p;
 }
 
@@ -279,7 +284,26 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
     }
   }
   const ProblemView& problem = problems[0];
-  const bool resident_ok = resident_supports(problem.ndim, d_.d1, d_.d2);
+  if (fp16_wave_variant()) {
+    // The reference's fp16 variants need power-of-two extents (its fp16
+    // cuFFT, src/cuda/cuda_solver.cu:74-80); here the fp16 storage runs on the
+    // register-resident and column passes, which take 16..1024 points.
+    if (options.amp_storage != AmpStorage::kF32) {
+      throw InvalidArgument("the half and mixed variants keep the amplitude in FP32");
+    }
+    for (int a = 0; a < ndim_; ++a) {
+      const long long len = problem.shape[a];
+      if (len < 16 || len > 1024 || (len & (len - 1)) != 0) {
+        throw InvalidArgument(
+            "the half and mixed variants need power-of-two extents of 16..1024 (fp16 storage)");
+      }
+    }
+    if (options.schedule == Schedule::kResident) {
+      throw InvalidArgument("the half and mixed variants run the streamed passes, not the "
+                            "resident schedule");
+    }
+  }
+  const bool resident_ok = resident_supports(problem.ndim, d_.d1, d_.d2) && !fp16_wave_variant();
   if (options.schedule == Schedule::kResident) {
     if (options.variant == Variant::kPlain) {
       throw InvalidArgument("the resident schedule runs batched starts only");
@@ -308,17 +332,30 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   if (resident_) batch_ = starts_;
   groups_ = starts_ / batch_;
   if (resident_) configure_resident();
+  iter_half_ = options.variant == Variant::kHalf;
+  wave_half_ = fp16_wave_variant();
+  if (fp16_wave_variant()) require_fp16_passes();
   options_.start = nullptr;
   amp_stride_ = problems_ > 1 ? n_ : 0;
 
-  const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
-  amp_tiled_ = fast_pass_lines(mod) > 0 && mod.S > 1 && !resident_;
+  // The modulus pass reads its amplitude tile by one bulk copy when the
+  // amplitude is stored in its CTA order: line-major for the TMA column pass,
+  // element-major for the register-resident pass.
+  PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
+  mod.amp_tiled = kAmpTiledLines;
+  if (!resident_ && column_pass_lines(mod, Mode::kMod) > 0) {
+    amp_tiled_ = kAmpTiledLines;
+  } else if (!resident_ && fast_pass_lines(mod) > 0 && mod.S > 1) {
+    amp_tiled_ = kAmpTiledElements;
+  }
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
   const std::size_t elem = options.amp_storage == AmpStorage::kF32 ? 4 : 2;
   amp_ = DeviceBuffer<unsigned char>(static_cast<std::size_t>(problems_) * n_ * elem);
   amp_f_ = DeviceBuffer<float>(static_cast<std::size_t>(problems_) * n_);
   support_ = DeviceBuffer<std::uint8_t>(total);
   x_ = DeviceBuffer<float2>(total);
+  if (iter_half_) xh_ = DeviceBuffer<std::uint32_t>(total);
+  if (fp16_wave_variant()) peaks_ = DeviceBuffer<float>(static_cast<std::size_t>(problems_));
   w_ = DeviceBuffer<float2>(total);
   saved_ = DeviceBuffer<std::uint8_t>(total);
   level_ = DeviceBuffer<LevelAcc>(static_cast<std::size_t>(starts_));
@@ -353,8 +390,11 @@ void Solver::reset(const std::vector<ProblemView>& problems, std::uint64_t seed,
 // captured graphs stay valid: every buffer keeps its address.
 void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
                   const float2* start) {
-  const PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
-  const int lines = amp_tiled_ ? fast_pass_lines(mod) : 0;
+  PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
+  mod.amp_tiled = amp_tiled_;
+  const int lines = amp_tiled_ == kAmpTiledLines     ? column_pass_lines(mod, Mode::kMod)
+                    : amp_tiled_ == kAmpTiledElements ? fast_pass_lines(mod)
+                                                      : 0;
   const std::size_t elem = options_.amp_storage == AmpStorage::kF32 ? 4 : 2;
   const std::size_t total = static_cast<std::size_t>(starts_) * n_;
   const bool on_device = problems[0].on_device;
@@ -396,14 +436,21 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
       v.on_device = true;
     }
     prepare_problem_device(v, d_, options_.amp_storage, mod.L, mod.S, lines,
+                           amp_tiled_ == kAmpTiledLines,
                            amp_f_.get() + static_cast<std::size_t>(q) * n_,
                            amp_.get() + static_cast<std::size_t>(q) * n_ * elem,
                            support_.get() + static_cast<std::size_t>(q) * spp_ * n_, region,
-                           energies + q, stream_);
+                           energies + q, fp16_wave_variant() ? peaks_.get() + q : nullptr,
+                           stream_);
   }
   energies_.assign(static_cast<std::size_t>(problems_), 0.0);
   QPB_CHECK(cudaMemcpyAsync(energies_.data(), energies, energies_.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, stream_));
+  amp_scale_.assign(static_cast<std::size_t>(problems_), 1.0f);
+  if (fp16_wave_variant()) {
+    QPB_CHECK(cudaMemcpyAsync(amp_scale_.data(), peaks_.get(), amp_scale_.size() * sizeof(float),
+                              cudaMemcpyDeviceToHost, stream_));
+  }
   QPB_CHECK(cudaMemsetAsync(x_.get(), 0, total * sizeof(float2), stream_));
   QPB_CHECK(cudaMemsetAsync(counters_.get(), 0, groups_ * sizeof(int), stream_));
   const Ctrl ctrl{nullptr, 0, 0.0f, 0.0f, counters_.get()};
@@ -424,21 +471,37 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
   iteration_ = 0;
   run_iterations_ = 0;
 
+  // The starts are made in complex64 (x_, and the wave buffer as complex64),
+  // as the reference makes an fp16 variant's starts in FP32 before rounding
+  // them (src/cuda/cuda_solver.cu:125-140); the storage flags are restored
+  // below, and an fp16 iterate is rounded from x_ at the end.
+  const bool wave_half = wave_half_;
+  const bool iter_half = iter_half_;
+  wave_half_ = false;
+  iter_half_ = false;
   if (start) {
-    // Given starts, centre-origin: to FFT order, cut to the support (cpu_solver.cpp:37-41).
+    // Given starts, centre-origin: to FFT order, cut to the support
+    // (cpu_solver.cpp:37-41), brought into the scale of an fp16 variant's
+    // amplitude (divided by its peak, as test_cuda.cpp:192-205 requires).
     QPB_CHECK(cudaMemcpyAsync(w_.get(), start, total * sizeof(float2), cudaMemcpyDefault,
                               stream_));
     roll<float2>(w_.get(), x_.get(), d_, starts_, true, stream_);
     support_project(x_.get(), support_.get(), n_, starts_, stream_);
+    if (fp16_wave_variant()) {
+      const std::size_t block = static_cast<std::size_t>(spp_) * n_;
+      for (int q = 0; q < problems_; ++q) {
+        scale_complex(x_.get() + q * block, static_cast<long long>(block),
+                      1.0f / amp_scale_[static_cast<std::size_t>(q)], stream_);
+      }
+    }
     wave_valid_ = false;
-    establish_wave();
   } else {
     // Random phases on the measured amplitude, inverse transform, cut to the
     // support (kernels.cpp:104-117): the inverse's last pass is an ER update.
     // A batched solver draws every start in one launch per pass (each start
     // keyed by its global index, as in its own group); the plain variant one
     // start per launch.
-    const bool together = options_.variant == Variant::kBatched;
+    const bool together = batched();
     const int chunks = together ? 1 : groups_;
     const int count = together ? starts_ : batch_;
     auto params = [&](Mode mode, int axis3, int g) {
@@ -462,6 +525,11 @@ void Solver::load(const std::vector<ProblemView>& problems, std::uint64_t seed,
     }
     wave_valid_ = true;
   }
+  wave_half_ = wave_half;
+  iter_half_ = iter_half;
+  if (iter_half_) to_half(x_.get(), xh_.get(), static_cast<long long>(total), stream_);
+  if (wave_half_) wave_valid_ = false;  // the complex64 wave of the starts is not the fp16 one
+  if (!wave_valid_) establish_wave();
   stream_.sync();
 }
 
@@ -485,9 +553,11 @@ PassParams Solver::base(Mode mode, int axis3, int g) const {
   p.coef_from_ctrl = 1;
   p.bump_counter = 1;
   p.amp_storage = options_.amp_storage;
-  p.amp_tiled = amp_tiled_ && mode == Mode::kMod ? 1 : 0;
+  p.amp_tiled = mode == Mode::kMod ? amp_tiled_ : 0;
   p.amp_stride = amp_stride_;
   p.starts_per_problem = spp_;
+  p.wave_half = wave_half_ ? 1 : 0;
+  p.iter_half = iter_half_ ? 1 : 0;
   return p;
 }
 
@@ -505,7 +575,7 @@ void Solver::enqueue_establish(int g, int count) {
 // A batched solver's starts in one launch per axis, whatever its groups; the
 // plain variant one start per launch like the rest of its iteration.
 void Solver::establish_wave() {
-  if (options_.variant == Variant::kBatched) {
+  if (batched()) {
     enqueue_establish(0, starts_);
   } else {
     for (int g = 0; g < groups_; ++g) enqueue_establish(g, batch_);
@@ -581,7 +651,42 @@ void Solver::apply(const OpDesc& o) {
 
 void Solver::end_run() {
   collect_errors(run_iterations_);
-  check_waits();
+  check_waits(plans_, stream_);
+}
+
+void Solver::require_fp16_passes() const {
+  struct Need {
+    Mode mode;
+    int axis3;
+  };
+  std::vector<Need> needs{{Mode::kMod, runner_.outer()}, {Mode::kUpd, 2}, {Mode::kFwdFromX, 2}};
+  if (runner_.has_mid()) {
+    needs.push_back({Mode::kInv, 1});
+    needs.push_back({Mode::kFwd, 1});
+  }
+  for (const Need& need : needs) {
+    // every launch size the solver uses: one group, and all starts at once
+    for (int count : {batch_, starts_}) {
+      PassParams p = runner_.params(need.mode, need.axis3, count);
+      p.wave_half = 1;
+      p.iter_half = options_.variant == Variant::kHalf ? 1 : 0;
+      p.amp_tiled = need.mode == Mode::kMod ? kAmpTiledLines : 0;
+      const bool column = column_pass_lines(p, need.mode) > 0;
+      p.amp_tiled = need.mode == Mode::kMod && p.S > 1 ? kAmpTiledElements : 0;
+      if (!column && !(fast_passes_enabled() && fast_pass_supports(p))) {
+        throw InvalidArgument("the half and mixed variants need the register-resident or column "
+                              "pass on every axis; this shape and start grouping have none on axis " +
+                              std::to_string(need.axis3 - (3 - ndim_)));
+      }
+    }
+  }
+}
+
+void Solver::set_wait(int tries, bool starve) {
+  if (tries < 1) throw InvalidArgument("the wait limit must be >= 1 poll");
+  stream_.sync();
+  graphs_.clear();
+  runner_.set_wait(tries, starve);
 }
 
 void Solver::run(const OpDesc* ops, std::size_t count) {
@@ -608,6 +713,16 @@ void Solver::run(const OpDesc* ops, std::size_t count) {
 }
 
 void Solver::begin_iterate(Coefficients c) {
+  if (options_.variant == Variant::kMixed) {
+    // The mixed variant's fp16 wave serves HIO and RAAR; ER (coefficients
+    // 0, 0) runs entirely in FP32 (the reference's src/cuda/cuda_solver.cu
+    // mixed path), so a stage boundary may change the wave's storage.
+    const bool half = !(c.a == 0.0f && c.b == 0.0f);
+    if (half != wave_half_) {
+      wave_half_ = half;
+      wave_valid_ = false;
+    }
+  }
   if (!wave_valid_) establish_wave();
   set_coefficients(ctrl_.get(), c.a, c.b, stream_);
 }
@@ -618,7 +733,7 @@ int Solver::chunk_length(int remaining) const {
 }
 
 void Solver::prepare_branches() {
-  if (groups_ > 1 && branches_.empty() && options_.variant == Variant::kBatched && !resident_) {
+  if (groups_ > 1 && branches_.empty() && batched() && !resident_) {
     // one branch stream per group plus a fork event and a join event per group
     for (int g = 0; g < groups_; ++g) branches_.push_back(std::make_unique<Stream>());
     branch_events_.resize(static_cast<std::size_t>(groups_) + 1);
@@ -633,7 +748,7 @@ void Solver::prepare_branches() {
 void Solver::enqueue_chunk_body(int len, cudaStream_t s) {
   if (resident_) {
     enqueue_chunk(len, s);
-  } else if (groups_ > 1 && options_.variant == Variant::kBatched) {
+  } else if (groups_ > 1 && batched()) {
     if (branches_.empty()) throw std::logic_error("prepare_branches() was not called");
     QPB_CHECK(cudaEventRecord(branch_events_[0], s));
     for (int g = 0; g < groups_; ++g) {
@@ -660,8 +775,10 @@ void Solver::iterate(int count, Coefficients c) {
   begin_iterate(c);
   for (int done = 0; done < count;) {
     const int len = chunk_length(count - done);
-    if (options_.variant == Variant::kBatched) {
-      auto it = graphs_.find(len);
+    if (batched()) {
+      // graphs by chunk length and wave storage (the mixed variant switches it)
+      const int key = 2 * len + (wave_half_ ? 1 : 0);
+      auto it = graphs_.find(key);
       trace("iterate chunk len=%d graph=%s", len, it == graphs_.end() ? "capture" : "cached");
       if (it == graphs_.end()) {
         prepare_branches();
@@ -679,7 +796,7 @@ void Solver::iterate(int count, Coefficients c) {
         QPB_CHECK(cudaStreamEndCapture(stream_, &graph));
         const unsigned long long kernels = launches() - before;
         count_launches(0ULL - kernels);  // counted again on every replay
-        it = graphs_.emplace(len, std::make_unique<Graph>(graph, kernels)).first;
+        it = graphs_.emplace(key, std::make_unique<Graph>(graph, kernels)).first;
       }
       it->second->launch(stream_);
     } else {
@@ -757,7 +874,7 @@ void Solver::shrinkwrap(const OpDesc& o) {
   // A batched solver blurs every start in one launch per axis (one level
   // accumulator per start), whatever its start groups; the plain variant
   // keeps one start per launch like the rest of its iteration.
-  const bool together = options_.variant == Variant::kBatched;
+  const bool together = batched();
   const int chunks = together ? 1 : groups_;
   const int count = together ? starts_ : batch_;
   auto params = [&](Mode mode, int axis3, int g) {
@@ -766,6 +883,10 @@ void Solver::shrinkwrap(const OpDesc& o) {
     p.blur_k = k;
     return p;
   };
+  // The blur runs in a complex64 wave whatever the wave's storage (an fp16
+  // iterate is widened as it is read); the wave is re-established afterwards.
+  const bool wave_half = wave_half_;
+  wave_half_ = false;
   for (int g = 0; g < chunks; ++g) {
     QPB_CHECK(cudaMemsetAsync(level_.get(), 0, count * sizeof(LevelAcc), stream_));
     runner_.launch(Mode::kBlurMag, outer, params(Mode::kBlurMag, outer, g), stream_);
@@ -776,6 +897,7 @@ void Solver::shrinkwrap(const OpDesc& o) {
     shrinkwrap_threshold(w(g), level_.get(), n_, count, o.method + 1, o.threshold, support(g),
                          stream_);
   }
+  wave_half_ = wave_half;
   wave_valid_ = false;
 }
 
@@ -827,8 +949,21 @@ void Solver::report() {
   progress_(progress_user_, iteration_, latest.data(), starts_);
 }
 
+void Solver::iterate_f32(float2* out) {
+  const std::size_t total = static_cast<std::size_t>(starts_) * n_;
+  if (iter_half_) from_half(xh_.get(), x_.get(), static_cast<long long>(total), stream_);
+  roll<float2>(x_.get(), out, d_, starts_, false, stream_);
+  if (fp16_wave_variant()) {
+    const std::size_t block = static_cast<std::size_t>(spp_) * n_;
+    for (int q = 0; q < problems_; ++q) {
+      scale_complex(out + q * block, static_cast<long long>(block),
+                    amp_scale_[static_cast<std::size_t>(q)], stream_);
+    }
+  }
+}
+
 void Solver::results_device(float2* objects, std::uint8_t* supports, float* errors) {
-  if (objects) roll<float2>(x_.get(), objects, d_, starts_, false, stream_);
+  if (objects) iterate_f32(objects);
   if (supports) roll<std::uint8_t>(support_.get(), supports, d_, starts_, false, stream_);
   stream_.sync();
   if (errors) {
@@ -859,7 +994,7 @@ void Solver::results_per_problem(float2* const* objects, std::uint8_t* const* su
   // straight into the caller's memory
   const std::size_t block = static_cast<std::size_t>(spp_) * n_;
   if (objects) {
-    roll<float2>(x_.get(), w_.get(), d_, starts_, false, stream_);
+    iterate_f32(w_.get());
     wave_valid_ = false;
     for (int q = 0; q < problems_; ++q) {
       if (!objects[q]) continue;
@@ -968,7 +1103,7 @@ float modulus_project(const ProblemView& problem, float2* obj, AmpStorage storag
                             cudaMemcpyDeviceToHost, ctx.stream));
   QPB_CHECK(cudaMemcpyAsync(&num, errs.get(), sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
   ctx.stream.sync();
-  check_waits();
+  check_waits(ctx.plans, ctx.stream);
   const auto centred = host_roll(host.data(), d, false);
   std::copy(centred.begin(), centred.end(), obj);
   return static_cast<float>(std::sqrt(num / (energy + kEps)));
@@ -1005,7 +1140,7 @@ void gaussian_blur(const float* image, int ndim, const long long* shape, float s
   QPB_CHECK(cudaMemcpyAsync(host.data(), w.get(), host.size() * sizeof(float2),
                             cudaMemcpyDeviceToHost, ctx.stream));
   ctx.stream.sync();
-  check_waits();
+  check_waits(ctx.plans, ctx.stream);
   for (long long i = 0; i < n; ++i) out[i] = host[i].x;
 }
 

@@ -27,7 +27,16 @@ class DeviceBuffer {
  public:
   DeviceBuffer() = default;
   explicit DeviceBuffer(std::size_t count) : count_(count) {
-    if (count) QPB_CHECK(cudaMalloc(reinterpret_cast<void**>(&ptr_), count * sizeof(T)));
+    if (!count) return;
+    const cudaError_t status = cudaMalloc(reinterpret_cast<void**>(&ptr_), count * sizeof(T));
+    if (status != cudaSuccess) {
+      // A failed allocation is not sticky, but it stays the thread's last
+      // error: clear it so that the next launch check does not report it.
+      (void)cudaGetLastError();
+      ptr_ = nullptr;
+      throw std::runtime_error("cudaMalloc of " + std::to_string(count * sizeof(T)) +
+                               " bytes: " + cudaGetErrorString(status));
+    }
   }
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
@@ -105,6 +114,13 @@ struct ProblemView {
 enum class Variant : int {
   kBatched = 0,  // `batch` starts per launch, iterations replayed from CUDA graphs
   kPlain = 1,    // one start per launch, launched directly: the in-repo baseline
+  // As kBatched with fp16 storage (the reference's Variant::half and ::mixed,
+  // solver.hpp:21-29, src/cuda/half.cu): kHalf keeps the iterate and the wave
+  // as fp16 pairs; kMixed keeps the wave in fp16 during HIO and RAAR and runs
+  // ER entirely in FP32, with an FP32 iterate throughout. Both divide the
+  // amplitude by its peak; power-of-two extents only.
+  kHalf = 2,
+  kMixed = 3,
 };
 
 // How batched iterations run.
@@ -157,8 +173,9 @@ struct OpDesc {
 
 using ProgressFn = void (*)(void* user, int iteration, const float* errors, int count);
 
-// Throws Timeout when a kernel's bounded wait gave up since the last check.
-void check_waits();
+// Throws Timeout when a line pass planned from `plans` gave up a bounded wait
+// since the last check (the work enqueued on `stream` so far included).
+void check_waits(PlanCache& plans, cudaStream_t stream);
 
 // Checks shape rank and extents; returns Dims3 (2D -> {1, ny, nx}).
 Dims3 dims_of(const ProblemView& p);
@@ -175,11 +192,21 @@ class PassRunner {
   int outer() const { return ndim_ == 2 ? 1 : 0; }
   bool has_mid() const { return ndim_ == 3; }
   Dims3 dims() const { return d_; }
+  // Polls a staged wait makes before giving up (kMaxWaitTries by default), and
+  // the timeout tests' fault injection (staged copies left out); both apply to
+  // passes whose parameters are made afterwards.
+  void set_wait(int tries, bool starve) {
+    wait_tries_ = tries;
+    starve_ = starve;
+  }
 
  private:
   Dims3 d_;
   int ndim_;
   const LinePlan* plans_[3];
+  int* wait_failures_;
+  int wait_tries_;
+  bool starve_ = false;
 };
 
 // Line plans shared by the single operators and the problem set-up, one cache
@@ -256,10 +283,33 @@ class Solver {
   void end_run();
   // The latest error of every start (after at least one iteration of this run).
   std::vector<float> latest_errors();
+  bool batched() const { return options_.variant != Variant::kPlain; }
+  bool wave_half() const { return wave_half_; }
+  bool fp16_wave_variant() const {
+    return options_.variant == Variant::kHalf || options_.variant == Variant::kMixed;
+  }
+  // Bounded waits: `tries` polls before a staged wait gives up; `starve`
+  // leaves the staged copies out so that every such wait runs out (the fault
+  // injection of the timeout tests; results are invalid and run() reports
+  // Timeout). Captured graphs are dropped so that the next chunks pick it up.
+  void set_wait(int tries, bool starve);
 
  private:
-  float2* x(int g) const { return x_.get() + static_cast<std::size_t>(g) * batch_ * n_; }
-  float2* w(int g) const { return w_.get() + static_cast<std::size_t>(g) * batch_ * n_; }
+  // The iterate of group g in its storage: complex64, or fp16 pairs (half variant).
+  float2* x(int g) const {
+    if (iter_half_) {
+      return reinterpret_cast<float2*>(xh_.get() + static_cast<std::size_t>(g) * batch_ * n_);
+    }
+    return x_.get() + static_cast<std::size_t>(g) * batch_ * n_;
+  }
+  // The wave of group g in its storage (fp16 pairs pack into the buffer's first half).
+  float2* w(int g) const {
+    if (wave_half_) {
+      return reinterpret_cast<float2*>(reinterpret_cast<std::uint32_t*>(w_.get()) +
+                                       static_cast<std::size_t>(g) * batch_ * n_);
+    }
+    return w_.get() + static_cast<std::size_t>(g) * batch_ * n_;
+  }
   std::uint8_t* support(int g) const {
     return support_.get() + static_cast<std::size_t>(g) * batch_ * n_;
   }
@@ -276,6 +326,13 @@ class Solver {
   void detwin_begin(int axis);
   void detwin_end();
   void collect_errors(int iterations);
+  // The power-of-two register-resident or column pass for every pass an fp16
+  // variant launches; InvalidArgument otherwise.
+  void require_fp16_passes() const;
+  // The complex64, unscaled iterate (centre-origin or FFT order as x_ holds
+  // it) into `out` (starts * numel): widened from fp16 and multiplied back by
+  // each problem's amplitude peak where the variant stores it so.
+  void iterate_f32(float2* out);
   void report();
   float to_error(double num, int start) const;
 
@@ -297,10 +354,15 @@ class Solver {
   DeviceBuffer<unsigned char> amp_;  // signed amplitude in the chosen storage
   DeviceBuffer<float> amp_f_;        // FP32 FFT-order amplitude, for the random starts
   DeviceBuffer<unsigned char> prep_;  // problem set-up: scratch, and host arrays staged
-  bool amp_tiled_ = false;           // amp_ in the modulus pass's CTA order
+  int amp_tiled_ = 0;                // amp_ in the modulus pass's CTA order (kAmpTiled*)
   bool resident_ = false;            // iterations run by the resident kernel
   DeviceBuffer<float2> x_;
-  DeviceBuffer<float2> w_;
+  DeviceBuffer<std::uint32_t> xh_;   // the half variant's fp16 iterate (one __half2 per element)
+  DeviceBuffer<float2> w_;           // the wave; fp16 pairs in its first half while wave_half_
+  DeviceBuffer<float> peaks_;        // per problem: the amplitude peak an fp16 variant divides by
+  std::vector<float> amp_scale_;     // host copy of peaks_ (1 without amplitude scaling)
+  bool wave_half_ = false;           // the wave is stored as fp16 pairs
+  bool iter_half_ = false;           // the iterate is stored as fp16 pairs (xh_)
   DeviceBuffer<std::uint8_t> support_;
   DeviceBuffer<std::uint8_t> saved_;
   DeviceBuffer<LevelAcc> level_;
@@ -310,7 +372,7 @@ class Solver {
   DeviceBuffer<double> errs_;
   int capacity_ = 0;
   bool wave_valid_ = false;
-  std::map<int, std::unique_ptr<Graph>> graphs_;
+  std::map<int, std::unique_ptr<Graph>> graphs_;  // by 2 * chunk length + wave_half_
   // Captured graphs run start groups as parallel branches, one stream each.
   std::vector<std::unique_ptr<Stream>> branches_;
   std::vector<cudaEvent_t> branch_events_;

@@ -30,8 +30,9 @@ namespace qpb {
 
 namespace {
 
-// device, d0, d1, d2, starts, storage, resident kernel among the candidates
-using Key = std::tuple<int, int, int, int, int, int, bool>;
+// device, d0, d1, d2, starts, amplitude storage, resident kernel among the
+// candidates, variant (fp16 storage changes the passes' cost)
+using Key = std::tuple<int, int, int, int, int, int, bool, int>;
 
 std::mutex g_mutex;
 std::map<Key, TunedSchedule> g_choice;
@@ -55,7 +56,7 @@ double time_candidate(const ProblemView& problem, const SolverOptions& base, int
   // replays the graphs the caller's run would replay; two chunks per timing
   // keep the host's share of the wall time small.
   o.sync_every = std::max(10, std::min(base.sync_every, 100));
-  o.variant = Variant::kBatched;
+  o.variant = base.variant == Variant::kPlain ? Variant::kBatched : base.variant;
   Solver solver(problem, o);
   const OpDesc raar{kOpRAAR, 2 * o.sync_every, 0.9f, 0.0f, 0.0f, 0, 0};
   solver.run(&raar, 1);  // captures the graph
@@ -79,7 +80,7 @@ TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& op
   int device = 0;
   QPB_CHECK(cudaGetDevice(&device));
   const Key key{device, d.d0, d.d1, d.d2, starts, static_cast<int>(options.amp_storage),
-                resident_ok};
+                resident_ok, static_cast<int>(options.variant)};
   std::lock_guard<std::mutex> lock(g_mutex);
   if (auto it = g_choice.find(key); it != g_choice.end()) return it->second;
   std::vector<int> candidates;
@@ -109,9 +110,13 @@ std::string tuning_report() {
   std::lock_guard<std::mutex> lock(g_mutex);
   std::ostringstream out;
   for (const auto& [key, choice] : g_choice) {
-    const auto& [device, d0, d1, d2, starts, storage, resident_ok] = key;
+    const auto& [device, d0, d1, d2, starts, storage, resident_ok, variant] = key;
     out << "device " << device << " shape " << d0 << "x" << d1 << "x" << d2 << " starts "
-        << starts << " storage " << storage << ": "
+        << starts << " storage " << storage
+        << (variant == static_cast<int>(Variant::kHalf)    ? " half"
+            : variant == static_cast<int>(Variant::kMixed) ? " mixed"
+                                                           : "")
+        << ": "
         << (choice.resident ? std::string("resident") : "batch " + std::to_string(choice.batch))
         << " (";
     bool first = true;
