@@ -8,6 +8,8 @@
 #include <stdexcept>
 #include <string>
 
+#include "nvtx_range.hpp"
+
 namespace qpb {
 
 BatchSolver::BatchSolver(const std::vector<ProblemView>& problems, const SolverOptions& options)
@@ -102,9 +104,11 @@ void BatchSolver::run(const OpDesc* ops, std::size_t count) {
     return;
   }
   validate_recipe(ops, count);
+  const NvtxRange recipe_range("batch recipe", recipe_iterations(ops, count));
   for (Class& c : classes_) c.solver->begin_run(ops, count);
   for (std::size_t i = 0; i < count; ++i) {
     const OpDesc& o = ops[i];
+    const NvtxRange stage_range(op_name(o.kind), o.n);
     Coefficients co{};
     switch (o.kind) {
       case kOpER:

@@ -43,29 +43,41 @@ namespace qpb {
 
 namespace {
 
-// CTA shape: LINES columns of L points, T threads a line, the wave stored as
-// WT (float2 or __half2). LINES = 8 gives 64-byte box rows for complex64
-// (SWIZZLE_64B) and 32-byte rows for fp16 pairs (SWIZZLE_32B); the register
-// budget is sized for MIN_CTAS resident CTAs per SM (registers <= 64K /
-// (NT * MIN_CTAS)).
-template <int L, class WT>
+// Lines per CTA of every column pass: 8 (the default), or 16 when the
+// environment sets QPB_COLUMN_LINES=16 (both are built; used to compare them).
+int column_lines() {
+  static const int lines = [] {
+    const char* v = std::getenv("QPB_COLUMN_LINES");
+    return v && std::atoi(v) == 16 ? 16 : 8;
+  }();
+  return lines;
+}
+
+// CTA shape: LINES_ columns of L points, T threads a line, the wave stored as
+// WT (float2 or __half2). A box row is LINES_ elements: 64 or 128 bytes of
+// complex64, 32 or 64 of fp16 pairs, swizzled with the pattern of that width.
+// The register budget is sized for MIN_CTAS resident CTAs per SM
+// (registers <= 64K / (NT * MIN_CTAS)): at 8 lines all CTAs of a 32-start
+// 256 x 256 launch fit in one wave.
+template <int L, class WT, int LINES_>
 struct ColumnTiling {
   using G = Geometry<L>;
-  static constexpr int LINES = 8;
+  static constexpr int LINES = LINES_;
   static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 64 ? 12 : 7;
+  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 7 : 3);
   static constexpr int ROW_BYTES = LINES * static_cast<int>(sizeof(WT));  // one box row
   static constexpr int kBox = L * ROW_BYTES;
   static constexpr int kExchange = LINES * G::PITCH * 8;
   static constexpr int kRegion = ((kBox > kExchange ? kBox : kExchange) + 1023) / 1024 * 1024;
-  static_assert(ROW_BYTES == 64 || ROW_BYTES == 32, "the swizzles below are the 64/32-byte patterns");
+  static_assert(ROW_BYTES == 128 || ROW_BYTES == 64 || ROW_BYTES == 32,
+                "the swizzles below are the 128/64/32-byte patterns");
   static_assert(G::T <= 32 && 32 % G::T == 0, "a line's threads must share one warp");
   static_assert(NT % 32 == 0, "whole warps");
 };
 
-template <int L, Mode M, class AmpT, class WT>
+template <int L, Mode M, class AmpT, class WT, int LINES>
 struct ColumnStaging {
-  using Ti = ColumnTiling<L, WT>;
+  using Ti = ColumnTiling<L, WT, LINES>;
   static constexpr bool kAmp = M == Mode::kMod;
   static constexpr int kAmpBytes = kAmp ? Ti::LINES * L * static_cast<int>(sizeof(AmpT)) : 0;
   static constexpr int kAmpOffset = Ti::kRegion;
@@ -76,12 +88,19 @@ struct ColumnStaging {
 };
 
 // Byte offset of logical byte `o` of a box in shared memory written with
-// CU_TENSOR_MAP_SWIZZLE_64B (16-byte chunk bits 4-5 XOR address bits 7-8) or
-// CU_TENSOR_MAP_SWIZZLE_32B (chunk bit 4 XOR address bit 7); the box starts
-// on a 1024-byte boundary.
+// CU_TENSOR_MAP_SWIZZLE_128B, _64B or _32B for box rows of that width (the
+// 16-byte chunk bits 4-6, 4-5 or 4 XOR address bits 7-9, 7-8 or 7); the box
+// starts on a 1024-byte boundary.
 template <int ROW_BYTES>
 __device__ __forceinline__ int swizzled(int o) {
-  return ROW_BYTES == 64 ? o ^ ((o >> 3) & 0x30) : o ^ ((o >> 3) & 0x10);
+  constexpr int mask = ROW_BYTES == 128 ? 0x70 : (ROW_BYTES == 64 ? 0x30 : 0x10);
+  return o ^ ((o >> 3) & mask);
+}
+
+template <int ROW_BYTES>
+constexpr CUtensorMapSwizzle swizzle_mode() {
+  return ROW_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                          : (ROW_BYTES == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1,
@@ -102,12 +121,13 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int
       : "memory");
 }
 
-template <int L, Mode M, class AmpT, class WT>
-__global__ void __launch_bounds__(ColumnTiling<L, WT>::NT, ColumnTiling<L, WT>::MIN_CTAS)
+template <int L, Mode M, class AmpT, class WT, int LINES_>
+__global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
+                                  ColumnTiling<L, WT, LINES_>::MIN_CTAS)
     column_pass_kernel(const __grid_constant__ CUtensorMap wmap, const PassParams p) {
   using G = Geometry<L>;
-  using Ti = ColumnTiling<L, WT>;
-  using St = ColumnStaging<L, M, AmpT, WT>;
+  using Ti = ColumnTiling<L, WT, LINES_>;
+  using St = ColumnStaging<L, M, AmpT, WT, LINES_>;
   constexpr int E = G::E;
   constexpr int T = G::T;
   constexpr int LINES = Ti::LINES;
@@ -226,9 +246,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // The launch's wave as a 3D tensor {S, L, outer slabs} of 8-byte (complex64)
 // or 4-byte (fp16 pair) elements and its [1][L][LINES] box.
-template <int L, class WT>
+template <int L, class WT, int LINES>
 CUtensorMap wave_map(const PassParams& p) {
-  using Ti = ColumnTiling<L, WT>;
+  using Ti = ColumnTiling<L, WT, LINES>;
   constexpr cuuint64_t kElem = sizeof(WT);
   CUtensorMap map{};
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(p.S), static_cast<cuuint64_t>(L),
@@ -240,7 +260,7 @@ CUtensorMap wave_map(const PassParams& p) {
   const CUresult r = encode_fn()(
       &map, kElem == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, p.w,
       dims, strides, box, estrides, CU_TENSOR_MAP_INTERLEAVE_NONE,
-      Ti::ROW_BYTES == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+      swizzle_mode<Ti::ROW_BYTES>(),
       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     throw std::runtime_error("cuTensorMapEncodeTiled failed for a column pass (code " +
@@ -249,15 +269,21 @@ CUtensorMap wave_map(const PassParams& p) {
   return map;
 }
 
-template <int L, Mode M, class AmpT, class WT>
-void launch_one(const PassParams& p, cudaStream_t stream) {
-  using Ti = ColumnTiling<L, WT>;
-  const CUtensorMap map = wave_map<L, WT>(p);
+template <int L, Mode M, class AmpT, class WT, int LINES>
+void launch_lines(const PassParams& p, cudaStream_t stream) {
+  using Ti = ColumnTiling<L, WT, LINES>;
+  const CUtensorMap map = wave_map<L, WT, LINES>(p);
   const dim3 grid(static_cast<unsigned>(p.lines / Ti::LINES));
-  column_pass_kernel<L, M, AmpT, WT>
-      <<<grid, Ti::NT, ColumnStaging<L, M, AmpT, WT>::kBytes, stream>>>(map, p);
+  column_pass_kernel<L, M, AmpT, WT, LINES>
+      <<<grid, Ti::NT, ColumnStaging<L, M, AmpT, WT, LINES>::kBytes, stream>>>(map, p);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
+}
+
+template <int L, Mode M, class AmpT, class WT>
+void launch_one(const PassParams& p, cudaStream_t stream) {
+  if (column_lines() == 16) return launch_lines<L, M, AmpT, WT, 16>(p, stream);
+  launch_lines<L, M, AmpT, WT, 8>(p, stream);
 }
 
 template <int L, Mode M>
@@ -296,13 +322,19 @@ void launch_length(Mode mode, const PassParams& p, cudaStream_t stream) {
   }
 }
 
-template <int L, Mode M, class AmpT, class WT = float2>
-void allow_one() {
-  constexpr int bytes = ColumnStaging<L, M, AmpT, WT>::kBytes;
+template <int L, Mode M, class AmpT, class WT, int LINES>
+void allow_lines() {
+  constexpr int bytes = ColumnStaging<L, M, AmpT, WT, LINES>::kBytes;
   if constexpr (bytes > 48 * 1024) {
-    QPB_CHECK(cudaFuncSetAttribute(column_pass_kernel<L, M, AmpT, WT>,
+    QPB_CHECK(cudaFuncSetAttribute(column_pass_kernel<L, M, AmpT, WT, LINES>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   }
+}
+
+template <int L, Mode M, class AmpT, class WT = float2>
+void allow_one() {
+  allow_lines<L, M, AmpT, WT, 8>();
+  allow_lines<L, M, AmpT, WT, 16>();
 }
 
 template <int L>
@@ -332,7 +364,7 @@ int column_pass_lines(const PassParams& p, Mode mode) {
   if (p.L != 64 && p.L != 128 && p.L != 256) return 0;
   if (mode != Mode::kMod && mode != Mode::kFwd && mode != Mode::kInv) return 0;
   if (mode == Mode::kMod && p.amp_tiled != kAmpTiledLines) return 0;
-  constexpr int lines = 8;  // ColumnTiling<L, WT>::LINES for every supported L and WT
+  const int lines = column_lines();
   if (p.S % lines != 0 || p.lines_per_start % lines != 0 || p.lines % lines != 0) return 0;
   if (p.lines % p.S != 0) return 0;
   if (reinterpret_cast<std::uintptr_t>(p.w) % 16 != 0) return 0;

@@ -23,6 +23,7 @@
 #include "column_pass.cuh"
 #include "device_setup.cuh"
 #include "fast_pass.cuh"
+#include "nvtx_range.hpp"
 #include "resident.cuh"
 #include "solver.hpp"
 
@@ -689,11 +690,25 @@ void Solver::set_wait(int tries, bool starve) {
   runner_.set_wait(tries, starve);
 }
 
+const char* op_name(int kind) {
+  switch (kind) {
+    case kOpER: return "ER";
+    case kOpHIO: return "HIO";
+    case kOpRAAR: return "RAAR";
+    case kOpShrinkwrap: return "Shrinkwrap";
+    case kOpDetwinBegin: return "DetwinBegin";
+    case kOpDetwinEnd: return "DetwinEnd";
+    default: return "op";
+  }
+}
+
 void Solver::run(const OpDesc* ops, std::size_t count) {
+  const NvtxRange recipe_range("recipe", recipe_iterations(ops, count));
   begin_run(ops, count);
   for (std::size_t i = 0; i < count; ++i) {
     const OpDesc& o = ops[i];
     trace("run op %zu/%zu kind=%d n=%d (iteration %d)", i, count, o.kind, o.n, iteration_);
+    const NvtxRange stage_range(op_name(o.kind), o.n);
     switch (o.kind) {
       case kOpER:
         iterate(o.n, er_coefficients());

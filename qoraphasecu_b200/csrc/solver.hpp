@@ -177,6 +177,9 @@ using ProgressFn = void (*)(void* user, int iteration, const float* errors, int 
 // since the last check (the work enqueued on `stream` so far included).
 void check_waits(PlanCache& plans, cudaStream_t stream);
 
+// The recipe operation's name ("ER", "RAAR", "Shrinkwrap", ...).
+const char* op_name(int kind);
+
 // Checks shape rank and extents; returns Dims3 (2D -> {1, ny, nx}).
 Dims3 dims_of(const ProblemView& p);
 void validate_recipe(const OpDesc* ops, std::size_t count);
