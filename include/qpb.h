@@ -241,15 +241,16 @@ QPB_API uint64_t qpb_kernel_launches(void);
  * which fixes the grouping through Options::batch (solver.hpp:44-46). */
 QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
 
-/* Runs `iterations` more iterations with every line pass launched directly
- * between CUDA events on the solver's stream, all queued behind a short hold
- * of the stream so that the device runs them back to back (the events time
- * the kernels, not the host's launch rate); ms_out[p] receives the mean
- * duration of pass p of one iteration (2D: modulus pass, update pass; 3D adds
- * the y-axis inverse and forward passes) and *n_passes their count (<= 8).
- * With the resident schedule, *n_passes = 1 and ms_out[0] is the mean time per
- * iteration of one launch running all `iterations`. Advances the iterate. No counterpart in the reference: it feeds the
- * per-kernel roofline that bench.py reports. */
+/* Times each line pass of an iteration: pass p is launched `iterations` times
+ * back to back (all start groups) between two CUDA events on the solver's
+ * stream, every launch queued behind a short hold of the stream so that the
+ * device runs them one after another (the events time the kernels, not the
+ * host's launch rate); ms_out[p] receives the mean time per launch and
+ * *n_passes their count (<= 8; 2D: modulus pass, update pass; 3D adds the
+ * y-axis inverse and forward passes). With the resident schedule, *n_passes =
+ * 1 and ms_out[0] is the mean time per iteration of one launch running all
+ * `iterations`. Changes the iterate. No counterpart in the reference: it
+ * feeds the per-kernel roofline that bench.py reports. */
 QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
 
 /* The modulus projection of qpb_modulus_project for callers that must not

@@ -447,11 +447,11 @@ class Solver:
         _lib.check(self._lib.qpb_set_wait_limit(self._handle, int(polls), int(bool(starve))))
 
     def profile_passes(self, iterations: int = 20):
-        """Mean device time (ms) of each line pass of one iteration, timed with
-        CUDA events around direct launches that the device runs back to back
-        (queued behind a short hold of the stream); with the resident schedule, one
-        value: the mean time per iteration of one launch of ``iterations``
-        iterations. Advances the iterate."""
+        """Mean device time (ms) per launch of each line pass of an iteration:
+        each pass launched ``iterations`` times back to back between two CUDA
+        events (queued behind a short hold of the stream); with the resident
+        schedule, one value: the mean time per iteration of one launch of
+        ``iterations`` iterations. Changes the iterate."""
         ms = (ctypes.c_double * 8)()
         n = ctypes.c_int()
         _lib.check(self._lib.qpb_profile_passes(self._handle, iterations, ms, ctypes.byref(n)))

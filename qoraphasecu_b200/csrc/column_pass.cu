@@ -5,7 +5,8 @@
 // launch's wave: {S, L, outer slabs}) brings the whole box into shared memory,
 // swizzled so that the row-order reads below are free of bank conflicts; a
 // modulus pass's amplitude tile (stored by the problem set-up in this pass's
-// CTA order, line-major) arrives by one bulk copy on the same mbarrier.
+// CTA order, line-major) and the transform's stage-major twiddle table arrive
+// by bulk copies on the same mbarrier.
 //
 // Inside the CTA the lines are held row-style: the T threads of a line sit in
 // one warp (thread t of line l owns elements t + T m), so every Stockham
@@ -81,10 +82,13 @@ struct ColumnStaging {
   static constexpr bool kAmp = M == Mode::kMod;
   static constexpr int kAmpBytes = kAmp ? Ti::LINES * L * static_cast<int>(sizeof(AmpT)) : 0;
   static constexpr int kAmpOffset = Ti::kRegion;
-  static constexpr int kBarrier = (kAmpOffset + kAmpBytes + 15) / 16 * 16;
+  // the stage-major twiddle table, copied next to the amplitude tile
+  static constexpr int kTwBytes = Ti::G::TW_COUNT * 8;
+  static constexpr int kTwOffset = kAmpOffset + kAmpBytes;
+  static constexpr int kBarrier = (kTwOffset + kTwBytes + 15) / 16 * 16;
   // + 1024: the dynamic shared memory base is aligned up to 1024 bytes inside
   static constexpr int kBytes = kBarrier + 16 + 1024;
-  static_assert(kAmpBytes % 16 == 0, "bulk copies need 16-byte sizes");
+  static_assert(kAmpBytes % 16 == 0 && kTwBytes % 16 == 0, "bulk copies need 16-byte sizes");
 };
 
 // Byte offset of logical byte `o` of a box in shared memory written with
@@ -147,9 +151,10 @@ __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
 
   if (tid == 0) {
     mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, St::kAmpBytes + Ti::kBox);
+    mbar_arrive_expect_tx(bar, St::kAmpBytes + St::kTwBytes + Ti::kBox);
     if (!p.starve) {
       tma_load_3d(box, &wmap, inner0, 0, outer, bar);
+      bulk_g2s(sbase + St::kTwOffset, p.stage_twiddle, St::kTwBytes, bar);
       if constexpr (St::kAmp) {
         const long long line_in_start =
             line0 - static_cast<long long>(batch_start) * p.lines_per_start;
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
                       : nullptr;
     }
   }
-  const float2* __restrict__ tw = p.stage_twiddle;
+  const float2* tw = reinterpret_cast<const float2*>(sbase + St::kTwOffset);
   __syncthreads();  // the barrier is initialised before anyone polls it
 
   if (!__syncthreads_and(mbar_wait(bar, 0, p.wait_tries) ? 1 : 0)) {
@@ -193,7 +198,7 @@ __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
   float2* row = reinterpret_cast<float2*>(box) + l * G::PITCH;
 
   if constexpr (M == Mode::kMod) {
-    transform<L, false, true, true>(v, t, tw, row);
+    transform<L, false, true, true, true>(v, t, tw, row);
     const AmpT* amp_tile = reinterpret_cast<const AmpT*>(sbase + St::kAmpOffset) + l * L;
     const float s = p.scale;
     float acc = 0.0f;
@@ -209,9 +214,9 @@ __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
       double* slot = *err_slot;
       if (slot) atomicAdd(slot, total);
     }
-    transform<L, true, true, true>(v, t, tw, row);
+    transform<L, true, true, true, true>(v, t, tw, row);
   } else {
-    transform<L, M == Mode::kInv, true, true>(v, t, tw, row);
+    transform<L, M == Mode::kInv, true, true, true>(v, t, tw, row);
   }
 
   __syncthreads();  // every line is done with the exchange rows

@@ -117,9 +117,12 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     base = outer * static_cast<long long>(L) * p.S + inner + static_cast<long long>(t) * p.S;
     step = T * p.S;
   }
-  // Not __restrict__: an operator may transform an array in place (w == x).
-  WT* wl = reinterpret_cast<WT*>(p.w) + base;
-  XT* xl = reinterpret_cast<XT*>(p.x) + base;
+  // Every mode that reads both x and w through these pointers (the column
+  // update and blur of |x|, the column forward from x) runs on distinct
+  // arrays; an operator that transforms in place (w == x) does so only in
+  // modes that reach x or w by bulk copies or through one of them.
+  WT* __restrict__ wl = reinterpret_cast<WT*>(p.w) + base;
+  XT* __restrict__ xl = reinterpret_cast<XT*>(p.x) + base;
   const float2* __restrict__ tw = p.stage_twiddle;
   // A row's T threads share a warp, so its exchanges need warp barriers only.
   constexpr bool kWarpLocal = ROWS && T <= 32;

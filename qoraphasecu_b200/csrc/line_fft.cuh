@@ -33,9 +33,11 @@ struct Geometry {
   static constexpr int R2 = L / (R0 * R1);
   static constexpr int STAGES = L <= 16 ? 1 : (R2 == 1 ? 2 : 3);
   static constexpr int PITCH = swz(L) + 1;
-  // Offsets of stages 1 and 2 in the stage-major twiddle table.
+  // Offsets of stages 1 and 2 in the stage-major twiddle table, and its size.
   static constexpr int OFF1 = 0;
   static constexpr int OFF2 = (R1 - 1) * R0;
+  static constexpr int TW_COUNT = (STAGES >= 2 ? (R1 - 1) * R0 : 0) +
+                                  (STAGES >= 3 ? (R2 - 1) * R0 * R1 : 0);
   static_assert(R0 * R1 * R2 == L, "bad factorisation");
   static_assert(R2 <= E && R1 <= E, "radix above the register count");
 };
@@ -73,8 +75,10 @@ __device__ __forceinline__ void line_sync() {
 // `tw` is the stage-major twiddle table (stage_twiddle_exponent): this
 // stage's W_L^{r k L/(NS R)} sits at tw[OFF + (r - 1) NS + k], so the
 // threads of a line, whose k are consecutive, read consecutive entries.
+// TW_SHARED: the table is a copy in shared memory (plain loads) instead of
+// global memory (read-only cached loads).
 template <int L, int R, int NS, int OFF, bool LAST, bool INV, bool WARP_LOCAL = false,
-          bool TRAIL = true>
+          bool TRAIL = true, bool TW_SHARED = false>
 __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
                                       const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
@@ -91,7 +95,7 @@ __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
     if constexpr (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const float2 w = __ldg(tw + OFF + (r - 1) * NS + k);
+        const float2 w = TW_SHARED ? tw[OFF + (r - 1) * NS + k] : __ldg(tw + OFF + (r - 1) * NS + k);
         u[r] = INV ? cmulc(u[r], w) : cmul(u[r], w);
       }
     }
@@ -120,20 +124,20 @@ __device__ __forceinline__ void stage(float2 (&v)[Geometry<L>::E], int t,
 // TRAIL false the transform returns without the barrier after its last
 // exchange: the caller must pass a block barrier before anything writes the
 // row again.
-template <int L, bool INV, bool WARP_LOCAL = false, bool TRAIL = true>
+template <int L, bool INV, bool WARP_LOCAL = false, bool TRAIL = true, bool TW_SHARED = false>
 __device__ __forceinline__ void transform(float2 (&v)[Geometry<L>::E], int t,
                                           const float2* __restrict__ tw, float2* row) {
   using G = Geometry<L>;
   static_assert(!WARP_LOCAL || G::T <= 32, "a line spans several warps");
   if constexpr (G::STAGES == 1) {
-    stage<L, G::R0, 1, 0, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, true, INV, WARP_LOCAL, true, TW_SHARED>(v, t, tw, row);
   } else if constexpr (G::STAGES == 2) {
-    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
-    stage<L, G::R1, G::R0, G::OFF1, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL, TRAIL, TW_SHARED>(v, t, tw, row);
+    stage<L, G::R1, G::R0, G::OFF1, true, INV, WARP_LOCAL, true, TW_SHARED>(v, t, tw, row);
   } else {
-    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL>(v, t, tw, row);
-    stage<L, G::R1, G::R0, G::OFF1, false, INV, WARP_LOCAL, TRAIL>(v, t, tw, row);
-    stage<L, G::R2, G::R0 * G::R1, G::OFF2, true, INV, WARP_LOCAL>(v, t, tw, row);
+    stage<L, G::R0, 1, 0, false, INV, WARP_LOCAL, true, TW_SHARED>(v, t, tw, row);
+    stage<L, G::R1, G::R0, G::OFF1, false, INV, WARP_LOCAL, TRAIL, TW_SHARED>(v, t, tw, row);
+    stage<L, G::R2, G::R0 * G::R1, G::OFF2, true, INV, WARP_LOCAL, true, TW_SHARED>(v, t, tw, row);
   }
 }
 

@@ -266,9 +266,9 @@ class Solver {
     progress_ = fn;
     progress_user_ = user;
   }
-  // Runs `iterations` iterations with every pass launched directly between
-  // CUDA events; ms[p] receives the mean duration of pass p of an iteration.
-  // Returns the number of passes per iteration (at most 8). Advances the state.
+  // Launches each pass of an iteration `iterations` times back to back between
+  // two CUDA events; ms[p] receives the mean time per launch of pass p.
+  // Returns the number of passes per iteration (at most 8). Changes the state.
   int profile_passes(int iterations, double* ms);
 
   // The steps of run(), for a driver that captures the chunks of several
