@@ -383,7 +383,7 @@ def tuned_batch(report):
             choice = line.split(key, 1)[1]
             if choice.startswith("batch "):
                 return int(choice.split()[1])
-            return "resident"
+            return choice.split()[0]  # "resident" or "persistent"
     return None
 
 
@@ -538,16 +538,18 @@ def workload_crystal(args):
     _, intensity = workloads.crystal(128, seed=3000)
     problem = qpc.make_problem(intensity)
     out = {}
-    for storage in ("f32", "f16"):
-        with qpc.Solver(problem, starts=4, seed=0, sync_every=50, amp_storage=storage) as s:
+    for name, kw in (("f32", dict(amp_storage="f32")), ("f16 amplitude", dict(amp_storage="f16")),
+                     ("half (fp16 iterate and wave)", dict(variant="half")),
+                     ("mixed (fp16 wave for HIO/RAAR)", dict(variant="mixed"))):
+        with qpc.Solver(problem, starts=4, seed=0, sync_every=50, **kw) as s:
             s.run(default_recipe())  # warm-up: tuning, graphs
             t0 = time.perf_counter()
             s.run(default_recipe())
             sec = time.perf_counter() - t0
             runs = s.results()
             pass_ms = s.profile_passes(5)
-        out[storage] = {"seconds": sec, "start_iterations_per_s": 4 * 720 / sec,
-                        "errors": [r.error for r in runs], "pass_ms": pass_ms}
+        out[name] = {"seconds": sec, "start_iterations_per_s": 4 * 720 / sec,
+                     "errors": [r.error for r in runs], "pass_ms": pass_ms}
     return {"workload": "crystal 128^3, Poisson 1e7, 4 starts, default_recipe (720 iterations, "
                         "continued from a first run)", "storage": out,
             "tuning": qpc.api.tuning_report().strip().splitlines()}
@@ -757,6 +759,22 @@ def main(argv=None):
             "batched_over_plain": value / plain_value,
             "f16_amplitude": {"value": world * STARTS * iters / (half_ms / 1e3), "ms_per_step": half_ms},
         }
+        # fp16 storage of the wave (and the iterate): the reference's half and
+        # mixed variants, same schedule choice by the autotuner.
+        for variant in ("half", "mixed"):
+            with qpc.Solver(problem, starts=STARTS, seed=seed, sync_every=args.sync_every,
+                            variant=variant, device=local, stream=stream.cuda_stream) as v:
+                v.run(recipe)
+                barrier()
+                e0.record(stream)
+                v.run(recipe)
+                e1.record(stream)
+                e1.synchronize()
+                v_ms = max_over_ranks(e0.elapsed_time(e1))
+                best = float(min(r.error for r in v.results()))
+            line["variants"][f"f16_wave_{variant}"] = {
+                "value": world * STARTS * iters / (v_ms / 1e3), "ms_per_step": v_ms,
+                "best_final_error": best}
 
         # End to end through the public API with host buffers: intensity from
         # pinned memory in, objects/supports/errors out, every step.

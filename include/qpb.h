@@ -61,11 +61,17 @@ typedef enum qpb_variant {
  * parallel graph branches. RESIDENT: square 2D problems of side 64, 128 or 256
  * only; each start's iterate stays in the shared memory of a thread-block
  * cluster for a whole chunk of sync_every iterations, one launch per chunk.
- * AUTO: the autotuner times the candidates once per shape and start count. */
+ * PERSISTENT: 2D problems with sides of 64, 128 or 256 (complex64 storage);
+ * a chunk of sync_every iterations of every start is one launch whose CTAs
+ * claim the passes' tiles from a work list, each tile waiting (bounded) only
+ * for the tiles of its own start that it reads, so the passes of different
+ * starts overlap with no launch boundary. AUTO: the autotuner times the
+ * candidates once per shape and start count. */
 typedef enum qpb_schedule {
   QPB_SCHEDULE_AUTO = 0,
   QPB_SCHEDULE_STREAMED = 1,
-  QPB_SCHEDULE_RESIDENT = 2
+  QPB_SCHEDULE_RESIDENT = 2,
+  QPB_SCHEDULE_PERSISTENT = 3
 } qpb_schedule;
 
 /* A made problem: the fields of qpcu::Problem (problem.hpp:26-31). */

@@ -30,7 +30,7 @@ OK, INVALID_ARGUMENT, RUNTIME_ERROR, TIMEOUT = 0, 1, 2, 3
 
 AMP_STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 VARIANTS = {"batched": 0, "plain": 1, "half": 2, "mixed": 3}
-SCHEDULES = {"auto": 0, "streamed": 1, "resident": 2}
+SCHEDULES = {"auto": 0, "streamed": 1, "resident": 2, "persistent": 3}
 OP_KINDS = {"er": 0, "hio": 1, "raar": 2, "shrinkwrap": 3, "detwin_begin": 4, "detwin_end": 5}
 METHODS = {"max": 0, "rms": 1}
 

@@ -378,7 +378,7 @@ class Solver:
                  variant: Literal["batched", "plain", "half", "mixed"] = "batched",
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
                  device: int = -1, stream: int | None = None,
-                 schedule: Literal["auto", "streamed", "resident"] = "auto"):
+                 schedule: Literal["auto", "streamed", "resident", "persistent"] = "auto"):
         self.problem = problem
         self.shape = problem.shape
         self._on_device = problem.on_device
@@ -526,7 +526,7 @@ class BatchSolver:
                  variant: Literal["batched", "plain", "half", "mixed"] = "batched",
                  amp_storage: Literal["f32", "f16", "bf16"] = "f32", progress=None,
                  device: int = -1, stream: int | None = None,
-                 schedule: Literal["auto", "streamed", "resident"] = "auto"):
+                 schedule: Literal["auto", "streamed", "resident", "persistent"] = "auto"):
         self.problems = list(problems)
         if not self.problems:
             raise ValueError("no problems")
@@ -701,7 +701,7 @@ def reconstruct(
     sync_every: int = 10,
     amp_storage: Literal["f32", "f16", "bf16"] = "f32",
     progress=None,
-    schedule: Literal["auto", "streamed", "resident"] = "auto",
+    schedule: Literal["auto", "streamed", "resident", "persistent"] = "auto",
 ) -> Reconstruction | Ensemble:
     """Array in, reconstruction out.
 
@@ -729,7 +729,9 @@ def reconstruct(
         progress: ``fn(iteration, errors)`` every ``sync_every`` iterations.
         schedule: how batched iterations run: ``"streamed"`` line passes,
             ``"resident"`` (square 2D of side 64, 128 or 256: each start held in
-            a thread-block cluster's shared memory) or ``"auto"`` (timed once
+            a thread-block cluster's shared memory), ``"persistent"`` (2D with
+            sides of 64, 128 or 256: a chunk of iterations of every start as
+            one launch walking a work list of tiles) or ``"auto"`` (timed once
             per shape and start count).
     """
     if _is_cuda_tensor(intensity):

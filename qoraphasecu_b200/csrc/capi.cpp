@@ -199,7 +199,7 @@ qpb::SolverOptions options_of(const qpb_options* options) {
   if (options->variant < QPB_VARIANT_BATCHED || options->variant > QPB_VARIANT_MIXED) {
     throw qpb::InvalidArgument("unknown variant");
   }
-  if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_RESIDENT) {
+  if (options->schedule < QPB_SCHEDULE_AUTO || options->schedule > QPB_SCHEDULE_PERSISTENT) {
     throw qpb::InvalidArgument("unknown schedule");
   }
   qpb::SolverOptions o;

@@ -1,21 +1,7 @@
-// Column line passes (stride S > 1) whose tiles move by TMA.
-//
-// A CTA owns LINES adjacent columns of one outer slab: a [L][LINES] complex64
-// box of the wave. One tensor-map copy (cp.async.bulk.tensor, 3D map over the
-// launch's wave: {S, L, outer slabs}) brings the whole box into shared memory,
-// swizzled so that the row-order reads below are free of bank conflicts; a
-// modulus pass's amplitude tile (stored by the problem set-up in this pass's
-// CTA order, line-major) and the transform's stage-major twiddle table arrive
-// by bulk copies on the same mbarrier.
-//
-// Inside the CTA the lines are held row-style: the T threads of a line sit in
-// one warp (thread t of line l owns elements t + T m), so every Stockham
-// exchange of the register-resident transform (line_fft.cuh) needs a warp
-// barrier only, and the Fourier-error sum is a warp reduction with one FP64
-// atomic per warp. The result goes back through the same swizzled box and
-// leaves by one tensor-map store. Block barriers: one after the box is read
-// into registers (the box becomes the exchange rows) and two around the
-// output box.
+// Column line passes (stride S > 1) whose tiles move by TMA: one tile of
+// column_tile.cuh per CTA (LINES adjacent columns as one [L][LINES] box of a
+// 3D tensor map over the launch's wave, {S, L, outer slabs}); this file holds
+// the kernel, the tensor-map encoding and the launch dispatch.
 //
 // Every wait is bounded (PassParams::wait_tries); a CTA that gives up waits
 // once more for its copies in flight, counts itself in p.wait_failures and
@@ -33,12 +19,8 @@
 #include <stdexcept>
 #include <string>
 
-#include "bulk_copy.cuh"
 #include "column_pass.cuh"
-#include "line_fft.cuh"
-#include "projection.cuh"
-#include "reduce.cuh"
-#include "storage.cuh"
+#include "column_tile.cuh"
 
 namespace qpb {
 
@@ -54,184 +36,25 @@ int column_lines() {
   return lines;
 }
 
-// CTA shape: LINES_ columns of L points, T threads a line, the wave stored as
-// WT (float2 or __half2). A box row is LINES_ elements: 64 or 128 bytes of
-// complex64, 32 or 64 of fp16 pairs, swizzled with the pattern of that width.
-// The register budget is sized for MIN_CTAS resident CTAs per SM
-// (registers <= 64K / (NT * MIN_CTAS)): at 8 lines all CTAs of a 32-start
-// 256 x 256 launch fit in one wave.
-template <int L, class WT, int LINES_>
-struct ColumnTiling {
-  using G = Geometry<L>;
-  static constexpr int LINES = LINES_;
-  static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 7 : 3);
-  static constexpr int ROW_BYTES = LINES * static_cast<int>(sizeof(WT));  // one box row
-  static constexpr int kBox = L * ROW_BYTES;
-  static constexpr int kExchange = LINES * G::PITCH * 8;
-  static constexpr int kRegion = ((kBox > kExchange ? kBox : kExchange) + 1023) / 1024 * 1024;
-  static_assert(ROW_BYTES == 128 || ROW_BYTES == 64 || ROW_BYTES == 32,
-                "the swizzles below are the 128/64/32-byte patterns");
-  static_assert(G::T <= 32 && 32 % G::T == 0, "a line's threads must share one warp");
-  static_assert(NT % 32 == 0, "whole warps");
-};
-
-template <int L, Mode M, class AmpT, class WT, int LINES>
-struct ColumnStaging {
-  using Ti = ColumnTiling<L, WT, LINES>;
-  static constexpr bool kAmp = M == Mode::kMod;
-  static constexpr int kAmpBytes = kAmp ? Ti::LINES * L * static_cast<int>(sizeof(AmpT)) : 0;
-  static constexpr int kAmpOffset = Ti::kRegion;
-  // the stage-major twiddle table, copied next to the amplitude tile
-  static constexpr int kTwBytes = Ti::G::TW_COUNT * 8;
-  static constexpr int kTwOffset = kAmpOffset + kAmpBytes;
-  static constexpr int kBarrier = (kTwOffset + kTwBytes + 15) / 16 * 16;
-  // + 1024: the dynamic shared memory base is aligned up to 1024 bytes inside
-  static constexpr int kBytes = kBarrier + 16 + 1024;
-  static_assert(kAmpBytes % 16 == 0 && kTwBytes % 16 == 0, "bulk copies need 16-byte sizes");
-};
-
-// Byte offset of logical byte `o` of a box in shared memory written with
-// CU_TENSOR_MAP_SWIZZLE_128B, _64B or _32B for box rows of that width (the
-// 16-byte chunk bits 4-6, 4-5 or 4 XOR address bits 7-9, 7-8 or 7); the box
-// starts on a 1024-byte boundary.
-template <int ROW_BYTES>
-__device__ __forceinline__ int swizzled(int o) {
-  constexpr int mask = ROW_BYTES == 128 ? 0x70 : (ROW_BYTES == 64 ? 0x30 : 0x10);
-  return o ^ ((o >> 3) & mask);
-}
-
-template <int ROW_BYTES>
-constexpr CUtensorMapSwizzle swizzle_mode() {
-  return ROW_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
-                          : (ROW_BYTES == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1,
-                                            int c2, std::uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
-      "l"(reinterpret_cast<std::uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int c1, int c2,
-                                             const void* src) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-          reinterpret_cast<std::uint64_t>(map)),
-      "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(src))
-      : "memory");
-}
-
+// One tile per CTA.
 template <int L, Mode M, class AmpT, class WT, int LINES_>
 __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT,
                                   ColumnTiling<L, WT, LINES_>::MIN_CTAS)
     column_pass_kernel(const __grid_constant__ CUtensorMap wmap, const PassParams p) {
-  using G = Geometry<L>;
-  using Ti = ColumnTiling<L, WT, LINES_>;
   using St = ColumnStaging<L, M, AmpT, WT, LINES_>;
-  constexpr int E = G::E;
-  constexpr int T = G::T;
-  constexpr int LINES = Ti::LINES;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sbase = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<std::uintptr_t>(smem_raw) + 1023) & ~static_cast<std::uintptr_t>(1023));
-  unsigned char* box = sbase;
-  auto* bar = reinterpret_cast<std::uint64_t*>(sbase + St::kBarrier);
-
-  const int tid = threadIdx.x;
-  const int l = tid / T;  // line within the CTA
-  const int t = tid % T;  // thread within the line
-  const long long line0 = static_cast<long long>(blockIdx.x) * LINES;
-  const int outer = static_cast<int>(line0 / p.S);
-  const int inner0 = static_cast<int>(line0 - static_cast<long long>(outer) * p.S);
-  const int batch_start = static_cast<int>(line0 / p.lines_per_start);
-
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, St::kAmpBytes + St::kTwBytes + Ti::kBox);
-    if (!p.starve) {
-      tma_load_3d(box, &wmap, inner0, 0, outer, bar);
-      bulk_g2s(sbase + St::kTwOffset, p.stage_twiddle, St::kTwBytes, bar);
-      if constexpr (St::kAmp) {
-        const long long line_in_start =
-            line0 - static_cast<long long>(batch_start) * p.lines_per_start;
-        const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
-                          line_in_start * L;
-        bulk_g2s(sbase + St::kAmpOffset, src, St::kAmpBytes, bar);
-      }
-    }
-  }
-  // Control values while the copies are in flight: a modulus pass's error
-  // row, kept in shared memory (next to the barrier) until the sum is ready.
-  auto* err_slot = reinterpret_cast<double**>(sbase + St::kBarrier + 8);
-  if constexpr (M == Mode::kMod) {
-    if (tid == 0) {
-      const Ctrl* c = p.ctrl;
-      const int r = c->counters[p.group];
-      *err_slot = r < c->capacity
-                      ? c->errs + static_cast<long long>(r) * p.starts_total + p.start0 + batch_start
-                      : nullptr;
-    }
-  }
-  const float2* tw = reinterpret_cast<const float2*>(sbase + St::kTwOffset);
+  ColumnSmem s;
+  s.box = sbase;
+  s.amp = sbase + St::kAmpOffset;
+  s.tw = reinterpret_cast<const float2*>(sbase + St::kTwOffset);
+  s.bar = reinterpret_cast<std::uint64_t*>(sbase + St::kBarrier);
+  s.err_slot = reinterpret_cast<double**>(sbase + St::kBarrier + 8);
+  if (threadIdx.x == 0) mbar_init(s.bar, 1);
   __syncthreads();  // the barrier is initialised before anyone polls it
-
-  if (!__syncthreads_and(mbar_wait(bar, 0, p.wait_tries) ? 1 : 0)) {
-    if (tid == 0) {
-      mbar_wait(bar, 0, p.wait_tries);  // copies still in flight land first
-      atomicAdd(p.wait_failures, 1);
-    }
-    return;
-  }
-
-  float2 v[E];
-#pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const int j = t + T * m;
-    v[m] = load_c(*reinterpret_cast<const WT*>(
-        box + swizzled<Ti::ROW_BYTES>(j * Ti::ROW_BYTES + l * static_cast<int>(sizeof(WT)))));
-  }
-  __syncthreads();  // the box becomes the lines' exchange rows
-  float2* row = reinterpret_cast<float2*>(box) + l * G::PITCH;
-
-  if constexpr (M == Mode::kMod) {
-    transform<L, false, true, true, true>(v, t, tw, row);
-    const AmpT* amp_tile = reinterpret_cast<const AmpT*>(sbase + St::kAmpOffset) + l * L;
-    const float s = p.scale;
-    float acc = 0.0f;
-#pragma unroll
-    for (int m = 0; m < E; ++m) {
-      // an fp16 wave defers the inverse's 1/sqrt(n) to the update pass
-      v[m] = pointwise_projection<Mode::kMod>(v[m], to_float(amp_tile[t + T * m]), s, acc,
-                                              kHalfStorage<WT> ? 1.0f : s);
-    }
-    // every line of the CTA belongs to one start: one atomic per warp
-    const double total = warp_sum_double(static_cast<double>(acc));
-    if ((tid & 31) == 0) {
-      double* slot = *err_slot;
-      if (slot) atomicAdd(slot, total);
-    }
-    transform<L, true, true, true, true>(v, t, tw, row);
-  } else {
-    transform<L, M == Mode::kInv, true, true, true>(v, t, tw, row);
-  }
-
-  __syncthreads();  // every line is done with the exchange rows
-#pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const int j = t + T * m;
-    *reinterpret_cast<WT*>(box + swizzled<Ti::ROW_BYTES>(
-        j * Ti::ROW_BYTES + l * static_cast<int>(sizeof(WT)))) = store_c<WT>(v[m]);
-  }
-  fence_proxy_async();
-  __syncthreads();
-  if (tid == 0) {
-    tma_store_3d(&wmap, inner0, 0, outer, box);
-    bulk_commit();
-    bulk_wait_reads();
+  if (column_tile<L, M, AmpT, WT, LINES_, true>(&wmap, p, blockIdx.x, s, 0, -1)) {
+    if (threadIdx.x == 0) bulk_wait_reads();
   }
 }
 
@@ -355,6 +178,21 @@ void allow_length() {
 }
 
 }  // namespace
+
+int column_pass_line_count() { return column_lines(); }
+
+CUtensorMap column_wave_map(const PassParams& p) {
+  switch (p.L) {
+    case 64:
+      return wave_map<64, float2, 8>(p);
+    case 128:
+      return wave_map<128, float2, 8>(p);
+    case 256:
+      return wave_map<256, float2, 8>(p);
+    default:
+      throw std::logic_error("column pass: unsupported length");
+  }
+}
 
 bool column_passes_enabled() {
   static const bool enabled = [] {

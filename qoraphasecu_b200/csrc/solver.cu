@@ -24,6 +24,7 @@
 #include "device_setup.cuh"
 #include "fast_pass.cuh"
 #include "nvtx_range.hpp"
+#include "persistent.cuh"
 #include "resident.cuh"
 #include "solver.hpp"
 
@@ -299,10 +300,16 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
             "the half and mixed variants need power-of-two extents of 16..1024 (fp16 storage)");
       }
     }
-    if (options.schedule == Schedule::kResident) {
+    if (options.schedule == Schedule::kResident || options.schedule == Schedule::kPersistent) {
       throw InvalidArgument("the half and mixed variants run the streamed passes, not the "
-                            "resident schedule");
+                            "resident or persistent schedule");
     }
+  }
+  const bool persistent_ok = options.variant == Variant::kBatched &&
+                             persistent_supports(problem.ndim, d_.d1, d_.d2);
+  if (options.schedule == Schedule::kPersistent && !persistent_ok) {
+    throw InvalidArgument("the persistent schedule runs batched complex64 starts of 2D problems "
+                          "with sides of 64, 128 or 256");
   }
   const bool resident_ok = resident_supports(problem.ndim, d_.d1, d_.d2) && !fp16_wave_variant();
   if (options.schedule == Schedule::kResident) {
@@ -317,22 +324,29 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
     batch_ = 1;
   } else if (options.schedule == Schedule::kResident) {
     resident_ = true;
+  } else if (options.schedule == Schedule::kPersistent) {
+    persistent_ = true;
   } else if (options.batch) {
     batch_ = options.batch;
   } else if (options.tune) {
     // Tuned on the first problem with every start: the work is the same.
     SolverOptions o = options;
     o.starts = starts_;
-    if (!resident_ok) o.schedule = Schedule::kStreamed;
+    if (!resident_ok && !persistent_ok) o.schedule = Schedule::kStreamed;
     const TunedSchedule t = tuned_schedule(problem, o);
     batch_ = t.batch;
-    resident_ = t.resident;
+    resident_ = t.resident && resident_ok;
+    persistent_ = t.persistent && persistent_ok;
   } else {
     batch_ = starts_;
   }
-  if (resident_) batch_ = starts_;
+  if (resident_ || persistent_) batch_ = starts_;
   groups_ = starts_ / batch_;
   if (resident_) configure_resident();
+  if (persistent_) {
+    configure_persistent();
+    work_ = DeviceBuffer<unsigned>(static_cast<std::size_t>(persistent_work_words(starts_)));
+  }
   iter_half_ = options.variant == Variant::kHalf;
   wave_half_ = fp16_wave_variant();
   if (fp16_wave_variant()) require_fp16_passes();
@@ -763,6 +777,11 @@ void Solver::prepare_branches() {
 void Solver::enqueue_chunk_body(int len, cudaStream_t s) {
   if (resident_) {
     enqueue_chunk(len, s);
+  } else if (persistent_) {
+    QPB_CHECK(cudaMemsetAsync(work_.get(), 0, work_.size() * sizeof(unsigned), s));
+    const int outer = runner_.outer();
+    launch_persistent(base(Mode::kMod, outer, 0), base(Mode::kUpd, 2, 0), starts_, len,
+                      work_.get(), s);
   } else if (groups_ > 1 && batched()) {
     if (branches_.empty()) throw std::logic_error("prepare_branches() was not called");
     QPB_CHECK(cudaEventRecord(branch_events_[0], s));
@@ -825,13 +844,13 @@ void Solver::iterate(int count, Coefficients c) {
 int Solver::profile_passes(int iterations, double* ms) {
   if (iterations < 1) throw InvalidArgument("iterations must be >= 1");
   if (!wave_valid_) establish_wave();
-  if (resident_) {
+  if (resident_ || persistent_) {
     // One launch of `iterations` iterations between two events.
     cudaEvent_t e0{}, e1{};
     QPB_CHECK(cudaEventCreate(&e0));
     QPB_CHECK(cudaEventCreate(&e1));
     QPB_CHECK(cudaEventRecord(e0, stream_));
-    enqueue_chunk(iterations, stream_);
+    enqueue_chunk_body(iterations, stream_);
     QPB_CHECK(cudaEventRecord(e1, stream_));
     stream_.sync();
     float t = 0.0f;

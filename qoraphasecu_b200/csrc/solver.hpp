@@ -125,9 +125,10 @@ enum class Variant : int {
 
 // How batched iterations run.
 enum class Schedule : int {
-  kAuto = 0,      // the autotuner picks (streamed groups or resident)
+  kAuto = 0,      // the autotuner picks (streamed groups, resident or persistent)
   kStreamed = 1,  // two (3D: four) streamed line passes per iteration, start groups as branches
   kResident = 2,  // one resident-cluster launch per chunk of iterations (square 2D, side 64/128/256)
+  kPersistent = 3,  // one work-list launch per chunk of iterations (2D, sides 64/128/256)
 };
 
 struct SolverOptions {
@@ -145,13 +146,15 @@ struct SolverOptions {
 };
 
 // The schedule the autotuner picks for this problem and start count: the
-// resident kernel (where it exists) or streamed passes with starts, starts/2,
-// starts/4 or starts/8 starts per launch (divisors only), timed once per
-// (device, shape, starts, amplitude storage) on scratch solvers and cached for
-// the process. QPB_TUNE=0 disables it (streamed, all starts in one launch).
+// resident kernel or the persistent kernel (where they exist) or streamed
+// passes with starts, starts/2, ..., starts/16 starts per launch (divisors
+// only), timed once per (device, shape, starts, amplitude storage, variant)
+// on scratch solvers and cached for the process. QPB_TUNE=0 disables it
+// (streamed, all starts in one launch).
 struct TunedSchedule {
   int batch;
   bool resident;
+  bool persistent = false;
 };
 TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& options);
 
@@ -247,6 +250,7 @@ class Solver {
   int starts() const { return starts_; }
   int problems() const { return problems_; }
   bool resident() const { return resident_; }
+  bool persistent() const { return persistent_; }
   int batch() const { return batch_; }
   long long numel() const { return n_; }
   int ndim() const { return ndim_; }
@@ -359,6 +363,8 @@ class Solver {
   DeviceBuffer<unsigned char> prep_;  // problem set-up: scratch, and host arrays staged
   int amp_tiled_ = 0;                // amp_ in the modulus pass's CTA order (kAmpTiled*)
   bool resident_ = false;            // iterations run by the resident kernel
+  bool persistent_ = false;          // iterations run by the persistent kernel
+  DeviceBuffer<unsigned> work_;      // the persistent kernel's work-list words
   DeviceBuffer<float2> x_;
   DeviceBuffer<std::uint32_t> xh_;   // the half variant's fp16 iterate (one __half2 per element)
   DeviceBuffer<float2> w_;           // the wave; fp16 pairs in its first half while wave_half_

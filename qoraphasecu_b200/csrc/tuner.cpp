@@ -23,6 +23,7 @@
 #include <tuple>
 #include <vector>
 
+#include "persistent.cuh"
 #include "resident.cuh"
 #include "solver.hpp"
 
@@ -44,10 +45,16 @@ bool tuning_enabled() {
   return !(v && *v == '0');
 }
 
+// batch > 0: streamed passes with that many starts per launch; 0: the
+// resident kernel; kPersistentCandidate: the persistent kernel.
+constexpr int kPersistentCandidate = -1;
+
 double time_candidate(const ProblemView& problem, const SolverOptions& base, int batch) {
   SolverOptions o = base;
-  o.batch = batch;
-  o.schedule = batch == 0 ? Schedule::kResident : Schedule::kStreamed;
+  o.batch = batch > 0 ? batch : 0;
+  o.schedule = batch == 0                      ? Schedule::kResident
+               : batch == kPersistentCandidate ? Schedule::kPersistent
+                                               : Schedule::kStreamed;
   o.tune = false;
   o.start = nullptr;
   o.seed = 0;
@@ -84,7 +91,13 @@ TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& op
   std::lock_guard<std::mutex> lock(g_mutex);
   if (auto it = g_choice.find(key); it != g_choice.end()) return it->second;
   std::vector<int> candidates;
-  if (resident_ok) candidates.push_back(0);
+  const bool resident_here = resident_ok && resident_supports(problem.ndim, d.d1, d.d2) &&
+                             options.variant == Variant::kBatched;
+  const bool persistent_here = options.schedule != Schedule::kStreamed &&
+                               options.variant == Variant::kBatched &&
+                               persistent_supports(problem.ndim, d.d1, d.d2);
+  if (resident_here) candidates.push_back(0);
+  if (persistent_here) candidates.push_back(kPersistentCandidate);
   for (int parts : {1, 2, 4, 8, 16}) {
     if (starts % parts == 0 && starts / parts >= 1) candidates.push_back(starts / parts);
   }
@@ -96,13 +109,15 @@ TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& op
     timings.emplace_back(batch, t);
     if (t < best_time * 0.98) {  // prefer earlier candidates unless clearly slower
       best_time = t;
-      best = batch == 0 ? TunedSchedule{starts, true} : TunedSchedule{batch, false};
+      best = batch == 0                      ? TunedSchedule{starts, true, false}
+             : batch == kPersistentCandidate ? TunedSchedule{starts, false, true}
+                                             : TunedSchedule{batch, false, false};
     }
   }
   g_choice[key] = best;
   g_timings[key] = timings;
   trace("tuned schedule for %dx%dx%d, %d starts: %s batch %d", d.d0, d.d1, d.d2, starts,
-        best.resident ? "resident" : "streamed", best.batch);
+        best.resident ? "resident" : (best.persistent ? "persistent" : "streamed"), best.batch);
   return best;
 }
 
@@ -117,13 +132,18 @@ std::string tuning_report() {
             : variant == static_cast<int>(Variant::kMixed) ? " mixed"
                                                            : "")
         << ": "
-        << (choice.resident ? std::string("resident") : "batch " + std::to_string(choice.batch))
+        << (choice.resident     ? std::string("resident")
+            : choice.persistent ? std::string("persistent")
+                                : "batch " + std::to_string(choice.batch))
         << " (";
     bool first = true;
     for (const auto& [batch, t] : g_timings[key]) {
       if (batch == 0) {
         out << (first ? "" : ", ") << "resident (" << resident_max_clusters(d2) << " clusters of "
             << resident_cluster(d2) << " CTAs at once): " << t * 1e3 << " ms";
+      } else if (batch == kPersistentCandidate) {
+        out << (first ? "" : ", ") << "persistent (" << persistent_grid(d1, d2)
+            << " CTAs): " << t * 1e3 << " ms";
       } else {
         out << (first ? "" : ", ") << batch << ": " << t * 1e3 << " ms";
       }
