@@ -14,10 +14,12 @@
 
 #include <cstdint>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 
 #include "column_pass.cuh"
 #include "column_tile.cuh"
@@ -97,10 +99,35 @@ CUtensorMap wave_map(const PassParams& p) {
   return map;
 }
 
+// Encoded tensor maps of this thread, by wave address and geometry: encoding
+// validates the whole description on the host, which a direct launch (the
+// plain variant, per-pass timing) would otherwise pay on every launch.
+struct MapKey {
+  const void* base;
+  long long lines;
+  int S, L, elem, lines_per_cta;
+  bool operator<(const MapKey& o) const {
+    return std::tie(base, lines, S, L, elem, lines_per_cta) <
+           std::tie(o.base, o.lines, o.S, o.L, o.elem, o.lines_per_cta);
+  }
+};
+
+template <int L, class WT, int LINES>
+const CUtensorMap& cached_wave_map(const PassParams& p) {
+  thread_local std::map<MapKey, CUtensorMap> cache;
+  const MapKey key{p.w, p.lines, p.S, L, static_cast<int>(sizeof(WT)), LINES};
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    if (cache.size() >= 256) cache.clear();  // buffers come and go; keep the cache small
+    it = cache.emplace(key, wave_map<L, WT, LINES>(p)).first;
+  }
+  return it->second;
+}
+
 template <int L, Mode M, class AmpT, class WT, int LINES>
 void launch_lines(const PassParams& p, cudaStream_t stream) {
   using Ti = ColumnTiling<L, WT, LINES>;
-  const CUtensorMap map = wave_map<L, WT, LINES>(p);
+  const CUtensorMap& map = cached_wave_map<L, WT, LINES>(p);
   const dim3 grid(static_cast<unsigned>(p.lines / Ti::LINES));
   column_pass_kernel<L, M, AmpT, WT, LINES>
       <<<grid, Ti::NT, ColumnStaging<L, M, AmpT, WT, LINES>::kBytes, stream>>>(map, p);
@@ -184,11 +211,11 @@ int column_pass_line_count() { return column_lines(); }
 CUtensorMap column_wave_map(const PassParams& p) {
   switch (p.L) {
     case 64:
-      return wave_map<64, float2, 8>(p);
+      return cached_wave_map<64, float2, 8>(p);
     case 128:
-      return wave_map<128, float2, 8>(p);
+      return cached_wave_map<128, float2, 8>(p);
     case 256:
-      return wave_map<256, float2, 8>(p);
+      return cached_wave_map<256, float2, 8>(p);
     default:
       throw std::logic_error("column pass: unsupported length");
   }

@@ -105,7 +105,16 @@ TunedSchedule tuned_schedule(const ProblemView& problem, const SolverOptions& op
   double best_time = 1e30;
   std::vector<std::pair<int, double>> timings;
   for (int batch : candidates) {
-    const double t = time_candidate(problem, options, batch);
+    double t = 0.0;
+    try {
+      t = time_candidate(problem, options, batch);
+    } catch (const Timeout&) {
+      throw;
+    } catch (const std::exception& e) {
+      // a candidate this device cannot run is left out
+      trace("tuner: candidate %d failed: %s", batch, e.what());
+      continue;
+    }
     timings.emplace_back(batch, t);
     if (t < best_time * 0.98) {  // prefer earlier candidates unless clearly slower
       best_time = t;
