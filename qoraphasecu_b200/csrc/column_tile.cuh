@@ -37,7 +37,7 @@ struct ColumnTiling {
   using G = Geometry<L>;
   static constexpr int LINES = LINES_;
   static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 7 : 3);
+  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 5 : 3);
   static constexpr int ROW_BYTES = LINES * static_cast<int>(sizeof(WT));  // one box row
   static constexpr int kBox = L * ROW_BYTES;
   static constexpr int kExchange = LINES * G::PITCH * 8;
@@ -107,21 +107,57 @@ struct ColumnSmem {
   double** err_slot;    // the modulus tile's error slot (thread 0 writes it)
 };
 
-// Tile `tile` of the pass described by `p` (lines tile * LINES ..), using
-// mbarrier phase `parity`. A modulus tile adds its Fourier-error numerator to
-// error row `err_row` (negative: the row the control block's counter of
-// p.group names). With LOAD_TW the tile also copies the twiddle table to
-// s.tw. The tile's tensor-map store is issued and committed by thread 0; the
-// caller waits for it (reads, or the whole write when other CTAs read the
-// result next). Returns false, after waiting once more for copies in flight
-// and counting the failure, when the staged wait gave up.
+// Tile `tile` of the pass described by `p` (lines tile * LINES ..) in two
+// halves. column_tile_issue (thread 0 only) starts the tile's copies on the
+// tile's mbarrier and, for a modulus tile, names its error slot: error row
+// `err_row` (negative: the row the control block's counter of p.group names).
+// With LOAD_TW it also copies the twiddle table to s.tw. column_tile_run (all
+// threads) waits for the copies with mbarrier phase `parity`, transforms,
+// projects and stores: thread 0 issues and commits the tile's tensor-map
+// store, which the caller waits for (its reads before the shared memory is
+// reused, its writes before other CTAs read the result). It returns false,
+// after waiting once more for copies in flight and counting the failure, when
+// the staged wait gave up.
 template <int L, Mode M, class AmpT, class WT, int LINES, bool LOAD_TW>
-__device__ __forceinline__ bool column_tile(const CUtensorMap* wmap, const PassParams& p,
-                                            long long tile, const ColumnSmem& s, unsigned parity,
-                                            int err_row) {
-  using G = Geometry<L>;
+__device__ __forceinline__ void column_tile_issue(const CUtensorMap* wmap, const PassParams& p,
+                                                  long long tile, const ColumnSmem& s,
+                                                  int err_row) {
   using Ti = ColumnTiling<L, WT, LINES>;
   using St = ColumnStaging<L, M, AmpT, WT, LINES>;
+  const long long line0 = tile * LINES;
+  const int outer = static_cast<int>(line0 / p.S);
+  const int inner0 = static_cast<int>(line0 - static_cast<long long>(outer) * p.S);
+  const int batch_start = static_cast<int>(line0 / p.lines_per_start);
+  mbar_arrive_expect_tx(s.bar, St::kAmpBytes + (LOAD_TW ? St::kTwBytes : 0) + Ti::kBox);
+  if (!p.starve) {
+    tma_load_3d(s.box, wmap, inner0, 0, outer, s.bar);
+    if constexpr (LOAD_TW) {
+      bulk_g2s(const_cast<float2*>(s.tw), p.stage_twiddle, St::kTwBytes, s.bar);
+    }
+    if constexpr (St::kAmp) {
+      const long long line_in_start =
+          line0 - static_cast<long long>(batch_start) * p.lines_per_start;
+      const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
+                        line_in_start * L;
+      bulk_g2s(s.amp, src, St::kAmpBytes, s.bar);
+    }
+  }
+  // control values while the copies are in flight: the error row
+  if constexpr (M == Mode::kMod) {
+    const Ctrl* c = p.ctrl;
+    const int r = err_row >= 0 ? err_row : c->counters[p.group];
+    *s.err_slot = r < c->capacity
+                      ? c->errs + static_cast<long long>(r) * p.starts_total + p.start0 + batch_start
+                      : nullptr;
+  }
+}
+
+template <int L, Mode M, class AmpT, class WT, int LINES>
+__device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const PassParams& p,
+                                                long long tile, const ColumnSmem& s,
+                                                unsigned parity) {
+  using G = Geometry<L>;
+  using Ti = ColumnTiling<L, WT, LINES>;
   constexpr int E = G::E;
   constexpr int T = G::T;
   const int tid = threadIdx.x;
@@ -130,32 +166,7 @@ __device__ __forceinline__ bool column_tile(const CUtensorMap* wmap, const PassP
   const long long line0 = tile * LINES;
   const int outer = static_cast<int>(line0 / p.S);
   const int inner0 = static_cast<int>(line0 - static_cast<long long>(outer) * p.S);
-  const int batch_start = static_cast<int>(line0 / p.lines_per_start);
 
-  if (tid == 0) {
-    mbar_arrive_expect_tx(s.bar, St::kAmpBytes + (LOAD_TW ? St::kTwBytes : 0) + Ti::kBox);
-    if (!p.starve) {
-      tma_load_3d(s.box, wmap, inner0, 0, outer, s.bar);
-      if constexpr (LOAD_TW) {
-        bulk_g2s(const_cast<float2*>(s.tw), p.stage_twiddle, St::kTwBytes, s.bar);
-      }
-      if constexpr (St::kAmp) {
-        const long long line_in_start =
-            line0 - static_cast<long long>(batch_start) * p.lines_per_start;
-        const AmpT* src = static_cast<const AmpT*>(p.amp) + amp_offset(p, p.start0 + batch_start) +
-                          line_in_start * L;
-        bulk_g2s(s.amp, src, St::kAmpBytes, s.bar);
-      }
-    }
-    // control values while the copies are in flight: the error row
-    if constexpr (M == Mode::kMod) {
-      const Ctrl* c = p.ctrl;
-      const int r = err_row >= 0 ? err_row : c->counters[p.group];
-      *s.err_slot = r < c->capacity ? c->errs + static_cast<long long>(r) * p.starts_total +
-                                          p.start0 + batch_start
-                                    : nullptr;
-    }
-  }
   if (!__syncthreads_and(mbar_wait(s.bar, parity, p.wait_tries) ? 1 : 0)) {
     if (tid == 0) {
       mbar_wait(s.bar, parity, p.wait_tries);  // copies still in flight land first
@@ -210,6 +221,15 @@ __device__ __forceinline__ bool column_tile(const CUtensorMap* wmap, const PassP
     bulk_commit();
   }
   return true;
+}
+
+// Both halves, for a CTA that runs one tile.
+template <int L, Mode M, class AmpT, class WT, int LINES, bool LOAD_TW>
+__device__ __forceinline__ bool column_tile(const CUtensorMap* wmap, const PassParams& p,
+                                            long long tile, const ColumnSmem& s, unsigned parity,
+                                            int err_row) {
+  if (threadIdx.x == 0) column_tile_issue<L, M, AmpT, WT, LINES, LOAD_TW>(wmap, p, tile, s, err_row);
+  return column_tile_run<L, M, AmpT, WT, LINES>(wmap, p, tile, s, parity);
 }
 
 }  // namespace qpb

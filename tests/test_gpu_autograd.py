@@ -106,3 +106,27 @@ def test_adam_with_support_projection_converges(gpu):
         assert run.errors.shape == (300,)
         assert run.errors[-1] < 0.5 * run.errors[0]
         assert np.all(run.object[~support.astype(bool)] == 0)
+
+
+def test_adam_magnitude_bound_keeps_masked_directions_in_check(gpu):
+    """Under a beamstop the loss leaves the masked Fourier components free;
+    the per-pixel bound keeps every start's object within `bound` RMS
+    amplitudes of the support, and the bounded run converges as far as the
+    unbounded one."""
+    from qoraphasecu_b200 import workloads
+
+    obj = workloads.square(128, seed=5)
+    intensity = np.abs(np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(obj), norm="ortho"))) ** 2
+    mask = workloads.beamstop(obj.shape, 4.0)
+    support = qpc.autocorrelation_support(intensity)
+    p = qpc.make_problem(intensity.astype(np.float32), support=support, mask=mask)
+    bounded = qad.adam_reconstruct(p, starts=4, steps=400, lr=2e-2, seed=1, bound=8.0)
+    free = qad.adam_reconstruct(p, starts=4, steps=400, lr=2e-2, seed=1, bound=None)
+    usable = mask == 0
+    inside = max(int(np.count_nonzero(support)), 1)
+    rms = np.sqrt(np.sum(intensity[usable].astype(np.float64)) / inside)
+    for b, f in zip(bounded, free, strict=True):
+        assert np.all(np.isfinite(b.object))
+        assert float(np.max(np.abs(b.object))) <= 8.0 * rms * (1 + 1e-5)
+        assert np.all(b.object[~support.astype(bool)] == 0)
+        assert b.errors[-1] <= f.errors[-1] * 1.25 + 1e-3
