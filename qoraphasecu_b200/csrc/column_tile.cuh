@@ -175,12 +175,15 @@ __device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const P
     return false;
   }
 
+  // Box byte offset of element t + T m of this thread's line: the swizzle
+  // repeats every 8 box rows and T is a multiple of 8, so the XOR bits are
+  // those of row t and the offset is this thread's one plus m T ROW_BYTES.
+  static_assert(T % 8 == 0, "the swizzle pattern must repeat every T rows");
+  const int lane_box = swizzled<Ti::ROW_BYTES>(t * Ti::ROW_BYTES + l * static_cast<int>(sizeof(WT)));
   float2 v[E];
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    const int j = t + T * m;
-    v[m] = load_c(*reinterpret_cast<const WT*>(
-        s.box + swizzled<Ti::ROW_BYTES>(j * Ti::ROW_BYTES + l * static_cast<int>(sizeof(WT)))));
+    v[m] = load_c(*reinterpret_cast<const WT*>(s.box + lane_box + m * T * Ti::ROW_BYTES));
   }
   __syncthreads();  // the box becomes the lines' exchange rows
   float2* row = reinterpret_cast<float2*>(s.box) + l * G::PITCH;
@@ -210,9 +213,7 @@ __device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const P
   __syncthreads();  // every line is done with the exchange rows
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    const int j = t + T * m;
-    *reinterpret_cast<WT*>(s.box + swizzled<Ti::ROW_BYTES>(
-        j * Ti::ROW_BYTES + l * static_cast<int>(sizeof(WT)))) = store_c<WT>(v[m]);
+    *reinterpret_cast<WT*>(s.box + lane_box + m * T * Ti::ROW_BYTES) = store_c<WT>(v[m]);
   }
   fence_proxy_async();
   __syncthreads();
