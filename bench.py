@@ -248,13 +248,15 @@ def run_reference(args):
 REFERENCE_GPU_VARIANTS = {"graph": 2, "batched": 3, "half": 4, "mixed": 6}  # qpcu::Variant
 
 
-def reference_gpu_baseline(intensity, mask, sync_every):
+def reference_gpu_baseline(intensity, mask, sync_every, *, starts=None, recipe=None):
     """The reference's own CUDA backend (src/cuda: cuFFT plans, its element-wise
     kernels, CUDA graphs) compiled from its sources (oracle/_ref/
     libqpcu_ref_cuda.so, cuFFT LTO callbacks off) on the same workload, timed
     as its bench/bench.cpp:33-45 does: per variant, one run of the whole recipe
     to warm up (plans, graphs), then one timed run, wall clock around run()
-    (which ends with the errors copied to the host)."""
+    (which ends with the errors copied to the host). Defaults: the benchmark's
+    32 starts and recipe; the support is the reference's autocorrelation
+    support (problem.cpp) unless the workload passes none either way."""
     import ctypes
 
     import numpy as np
@@ -267,17 +269,21 @@ def reference_gpu_baseline(intensity, mask, sync_every):
     lib = oracle_ref.load_variant("cuda")
     if not lib.qref_cuda_available():
         return {"unavailable": "no CUDA device"}
+    starts = starts or STARTS
+    recipe = recipe or workloads.gaussians_recipe()
+    iterations = recipe.iterations()
     amp, msk, sup = oracle_ref.make_problem(intensity, None, mask)
-    ops = oracle_ref._ops(workloads.gaussians_recipe().ops())
-    count = len(workloads.gaussians_recipe().ops())
+    ops = oracle_ref._ops(recipe.ops())
+    count = len(recipe.ops())
     out = {"source": "QoraPhaseCU src/cuda compiled from its sources (nvcc sm_100a, cuFFT "
-                     "11.4, LTO callbacks off)", "starts": STARTS, "sync_every": sync_every}
+                     "11.4, LTO callbacks off)", "starts": starts, "sync_every": sync_every}
     for name, variant in REFERENCE_GPU_VARIANTS.items():
         handle = ctypes.c_void_p()
         status = lib.qref_create_backend(oracle_ref._p(amp), oracle_ref._p(msk),
-                                         oracle_ref._p(sup), 2, oracle_ref._shape(amp.shape),
-                                         STARTS, ctypes.c_uint64(0), None, sync_every, 1,
-                                         variant, 0, ctypes.byref(handle))
+                                         oracle_ref._p(sup), amp.ndim,
+                                         oracle_ref._shape(amp.shape), starts,
+                                         ctypes.c_uint64(0), None, sync_every, 1, variant, 0,
+                                         ctypes.byref(handle))
         if status:
             out[name] = {"error": lib.qref_last_error().decode()}
             continue
@@ -292,11 +298,11 @@ def reference_gpu_baseline(intensity, mask, sync_every):
                 out[name] = {"error": lib.qref_last_error().decode()}
                 continue
             n_err = lib.qref_error_count(handle)
-            errors = np.empty((STARTS, n_err), np.float32)
+            errors = np.empty((starts, n_err), np.float32)
             lib.qref_results(handle, None, None, oracle_ref._p(errors),
                              ctypes.byref(ctypes.c_size_t()))
-            out[name] = {"value": STARTS * 700 / seconds, "unit": UNIT,
-                         "us_per_iteration": seconds / 700 * 1e6,
+            out[name] = {"value": starts * iterations / seconds, "unit": UNIT,
+                         "us_per_iteration": seconds / iterations * 1e6,
                          "best_final_error": float(errors[:, -1].min())}
         finally:
             lib.qref_destroy(handle)
@@ -563,8 +569,10 @@ def workload_crystal(args):
             pass_ms = s.profile_passes(5)
         out[name] = {"seconds": sec, "start_iterations_per_s": 4 * 720 / sec,
                      "errors": [r.error for r in runs], "pass_ms": pass_ms}
+    reference = reference_gpu_baseline(intensity, None, 50, starts=4, recipe=default_recipe())
     return {"workload": "crystal 128^3, Poisson 1e7, 4 starts, default_recipe (720 iterations, "
                         "continued from a first run)", "storage": out,
+            "reference_gpu_baseline": reference,
             "tuning": qpc.api.tuning_report().strip().splitlines()}
 
 
