@@ -241,6 +241,10 @@ int column_pass_lines(const PassParams& p, Mode mode) {
   return lines;
 }
 
+bool column_pass_preferred(const PassParams& p, Mode mode) {
+  return p.L >= 256 && column_pass_lines(p, mode) > 0;
+}
+
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
   switch (p.L) {
     case 64:

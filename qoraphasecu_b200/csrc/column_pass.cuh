@@ -19,6 +19,14 @@ bool column_passes_enabled();
 // pass's CTA order), kFwd and kInv.
 int column_pass_lines(const PassParams& p, Mode mode);
 
+// True where the TMA column pass is the one to run on this column axis: it can
+// (column_pass_lines) and its lines have 256 points. Lines of 64 and 128 points
+// run the register-resident column pass, which measured faster there (the
+// 128^3 crystal's z and y passes: 42.8 / 23.6 / 22.6 us against 45.7 / 25.2 /
+// 25.7 us); at 256 the TMA pass is faster (the 256^2 benchmark's modulus pass:
+// 14.2 against 14.6 us, its step 12.2 against 12.8 ms).
+bool column_pass_preferred(const PassParams& p, Mode mode);
+
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream);
 
 // Lines per CTA of the column passes (8, or 16 when the environment sets

@@ -366,7 +366,11 @@ int choose_lpc(int L, int S, int lines_per_start) {
 }
 
 void launch_line_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
-  if (column_pass_lines(p, mode) > 0) return launch_column_pass(mode, p, stream);
+  // a modulus pass follows the amplitude's layout, which the solver chose
+  // with column_pass_preferred (or for the persistent schedule's column tiles)
+  if (mode == Mode::kMod ? column_pass_lines(p, mode) > 0 : column_pass_preferred(p, mode)) {
+    return launch_column_pass(mode, p, stream);
+  }
   if (p.amp_tiled == kAmpTiledLines) {
     throw std::logic_error("line pass: a line-major tiled amplitude needs the column pass");
   }

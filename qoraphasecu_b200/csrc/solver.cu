@@ -354,11 +354,13 @@ Solver::Solver(const std::vector<ProblemView>& problems, const SolverOptions& op
   amp_stride_ = problems_ > 1 ? n_ : 0;
 
   // The modulus pass reads its amplitude tile by one bulk copy when the
-  // amplitude is stored in its CTA order: line-major for the TMA column pass,
-  // element-major for the register-resident pass.
+  // amplitude is stored in its CTA order: line-major for the TMA column pass
+  // (where it is preferred, and always for the persistent kernel's column
+  // tiles), element-major for the register-resident pass.
   PassParams mod = runner_.params(Mode::kMod, runner_.outer(), batch_);
   mod.amp_tiled = kAmpTiledLines;
-  if (!resident_ && column_pass_lines(mod, Mode::kMod) > 0) {
+  if (!resident_ && (persistent_ ? column_pass_lines(mod, Mode::kMod) > 0
+                                 : column_pass_preferred(mod, Mode::kMod))) {
     amp_tiled_ = kAmpTiledLines;
   } else if (!resident_ && fast_pass_lines(mod) > 0 && mod.S > 1) {
     amp_tiled_ = kAmpTiledElements;
