@@ -29,10 +29,6 @@ bool column_pass_preferred(const PassParams& p, Mode mode);
 
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream);
 
-// Lines per CTA of the column passes (8, or 16 when the environment sets
-// QPB_COLUMN_LINES=16).
-int column_pass_line_count();
-
 // The tensor map of a complex64 wave that column tiles of 8 lines move:
 // p.w as {S, L, p.lines / S} elements, box [1][L][8], 64-byte swizzle.
 CUtensorMap column_wave_map(const PassParams& p);

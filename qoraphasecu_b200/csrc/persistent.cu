@@ -387,8 +387,7 @@ int grid_y(int lx) {
 
 bool persistent_supports(int ndim, int d1, int d2) {
   auto side = [](int n) { return n == 64 || n == 128 || n == 256; };
-  return ndim == 2 && side(d1) && side(d2) && column_passes_enabled() &&
-         column_pass_line_count() == kColumnLines;
+  return ndim == 2 && side(d1) && side(d2) && column_passes_enabled();
 }
 
 void launch_persistent(const PassParams& mod, const PassParams& upd, int starts, int iterations,
