@@ -683,6 +683,19 @@ def main(argv=None):
         single.run(workloads.hio_recipe(5))
         pass_ms = single.profile_passes(20)
     elems = STARTS * SHAPE[0] * SHAPE[1]
+    # The same two kernels on more starts of the problem, whose iterate and
+    # wave (128 starts: 134 MB; 512 starts: 537 MB) no longer fit in L2: one
+    # launch per pass, outside the timed region.
+    beyond_l2 = []
+    for starts in (128, 512):
+        with qpc.Solver(problem, starts=starts, seed=seed, batch=starts, device=local,
+                        stream=stream.cuda_stream) as big:
+            big.run(workloads.hio_recipe(5))
+            big_ms = big.profile_passes(20)
+        n_big = starts * SHAPE[0] * SHAPE[1]
+        beyond_l2.append({"starts": starts, **{
+            name.split(" ")[0]: {"ms": ms, "gbs": bpe * n_big / (ms * 1e6)}
+            for (name, bpe), ms in zip(PASS_BYTES.items(), big_ms)}})
     passes = []
     for (name, bpe), ms in zip(PASS_BYTES.items(), pass_ms):
         unfused = UNFUSED_BYTES[name] * elems
@@ -722,6 +735,7 @@ def main(argv=None):
             "achieved_pass_gbs": fused_bytes / (iter_ms * 1e6),
         },
         "note": "32 starts x 256^2 (16 MiB iterate) stay L2-resident across an iteration",
+        "passes_beyond_l2": beyond_l2,
     }
 
     line = {
