@@ -248,10 +248,11 @@ QPB_API uint64_t qpb_kernel_launches(void);
 QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
 
 /* Times each line pass of an iteration: pass p is launched `iterations` times
- * back to back (all start groups) between two CUDA events on the solver's
- * stream, every launch queued behind a short hold of the stream so that the
- * device runs them one after another (the events time the kernels, not the
- * host's launch rate); ms_out[p] receives the mean time per launch and
+ * back to back (all start groups) from one captured CUDA graph, replayed once
+ * untimed and once between two CUDA events on the solver's stream (the events
+ * time the kernels, not the host's launch rate; the solver's stream must be
+ * capturable, not the legacy default stream); ms_out[p] receives the mean time
+ * per launch and
  * *n_passes their count (<= 8; 2D: modulus pass, update pass; 3D adds the
  * y-axis inverse and forward passes). With the resident schedule, *n_passes =
  * 1 and ms_out[0] is the mean time per iteration of one launch running all

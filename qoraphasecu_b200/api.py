@@ -448,8 +448,8 @@ class Solver:
 
     def profile_passes(self, iterations: int = 20):
         """Mean device time (ms) per launch of each line pass of an iteration:
-        each pass launched ``iterations`` times back to back between two CUDA
-        events (queued behind a short hold of the stream); with the resident
+        each pass launched ``iterations`` times back to back from one captured
+        CUDA graph, whose replay two CUDA events time; with the resident
         schedule, one value: the mean time per iteration of one launch of
         ``iterations`` iterations. Changes the iterate."""
         ms = (ctypes.c_double * 8)()

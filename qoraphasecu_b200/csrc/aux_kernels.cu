@@ -146,18 +146,6 @@ __global__ void from_half_kernel(const __half2* in, float2* out, long long count
   QPB_FOR(i, count) { out[i] = __half22float2(in[i]); }
 }
 
-// Occupies the stream for about `ns` nanoseconds of the device's global
-// timer, sleeping between reads; at most 4096 sleeps of 1 us, so it ends.
-__global__ void hold_stream_kernel(long long ns) {
-  unsigned long long t0 = 0, t = 0;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-  for (int i = 0; i < 4096; ++i) {
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    if (static_cast<long long>(t - t0) >= ns) break;
-    __nanosleep(1000);
-  }
-}
-
 dim3 grid(long long n, int batch) {
   return {static_cast<unsigned>(blocks_for(n)), static_cast<unsigned>(batch), 1};
 }
@@ -171,12 +159,6 @@ void random_wave(float2* w, const float* amplitude, long long amp_stride, int st
   random_wave_kernel<<<grid(n, batch), kThreads, 0, stream>>>(w, amplitude, amp_stride,
                                                               starts_per_problem, n, seed,
                                                               first_start);
-  QPB_CHECK(cudaGetLastError());
-  count_launches(1);
-}
-
-void hold_stream(long long ns, cudaStream_t stream) {
-  hold_stream_kernel<<<1, 32, 0, stream>>>(ns);
   QPB_CHECK(cudaGetLastError());
   count_launches(1);
 }

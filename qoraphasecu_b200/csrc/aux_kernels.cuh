@@ -55,9 +55,4 @@ void scale_complex(float2* x, long long count, float scale, cudaStream_t stream)
 void to_half(const float2* in, void* out, long long count, cudaStream_t stream);
 void from_half(const void* in, float2* out, long long count, cudaStream_t stream);
 
-// Keeps `stream` busy for about `ns` nanoseconds (at most about 4 ms), so that
-// the host can queue timed work behind it and the device then runs that work
-// back to back, its events timing the kernels rather than the host's launches.
-void hold_stream(long long ns, cudaStream_t stream);
-
 }  // namespace qpb
