@@ -40,7 +40,11 @@ struct ColumnTiling {
   static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 5 : 3);
   static constexpr int ROW_BYTES = LINES * static_cast<int>(sizeof(WT));  // one box row
   static constexpr int kBox = L * ROW_BYTES;
-  static constexpr int kExchange = LINES * G::PITCH * 8;
+  // A half-warp holds 8 threads of each of two lines (column_tile_run); their
+  // exchange rows sit 8 mod 16 complex values apart so that the two lines'
+  // accesses fall on disjoint banks.
+  static constexpr int PITCH = (G::PITCH + 7) / 16 * 16 + 8;
+  static constexpr int kExchange = LINES * PITCH * 8;
   // the box, later the lines' exchange rows; a multiple of 1024 bytes
   static constexpr int kRegion = ((kBox > kExchange ? kBox : kExchange) + 1023) / 1024 * 1024;
   static_assert(ROW_BYTES == 128 || ROW_BYTES == 64 || ROW_BYTES == 32,
@@ -161,8 +165,14 @@ __device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const P
   constexpr int E = G::E;
   constexpr int T = G::T;
   const int tid = threadIdx.x;
-  const int l = tid / T;  // line within the tile
-  const int t = tid % T;  // thread within the line
+  // Line l and thread t of the line: with 16 threads a line, a half-warp
+  // holds threads t = 8 h .. 8 h + 7 of two lines (lane = 16 h + 8 (l & 1) +
+  // t mod 8), so that each 64-bit half-warp access of the swizzled box touches
+  // 8 rows of 2 columns, 16 distinct 8-byte slots; shorter lines hold 8
+  // threads, already 2 lines a half-warp (lane = 8 (l mod 4) + t).
+  const int lane = tid & 31;
+  const int l = T == 16 ? (tid >> 5) * 2 + ((lane >> 3) & 1) : tid / T;
+  const int t = T == 16 ? (lane >> 4) * 8 + (lane & 7) : tid % T;
   const long long line0 = tile * LINES;
   const int outer = static_cast<int>(line0 / p.S);
   const int inner0 = static_cast<int>(line0 - static_cast<long long>(outer) * p.S);
@@ -186,18 +196,20 @@ __device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const P
     v[m] = load_c(*reinterpret_cast<const WT*>(s.box + lane_box + m * T * Ti::ROW_BYTES));
   }
   __syncthreads();  // the box becomes the lines' exchange rows
-  float2* row = reinterpret_cast<float2*>(s.box) + l * G::PITCH;
+  float2* row = reinterpret_cast<float2*>(s.box) + l * Ti::PITCH;
 
   if constexpr (M == Mode::kMod) {
     transform<L, false, true, true, true>(v, t, s.tw, row);
+    // line l of the tile is stored rotated by amp_line_rotation(L, l)
     const AmpT* amp_tile = static_cast<const AmpT*>(s.amp) + l * L;
+    const int rot = amp_line_rotation(L, l);
     const float sc = p.scale;
     float acc = 0.0f;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       // an fp16 wave defers the inverse's 1/sqrt(n) to the update pass
-      v[m] = pointwise_projection<Mode::kMod>(v[m], to_float(amp_tile[t + T * m]), sc, acc,
-                                              kHalfStorage<WT> ? 1.0f : sc);
+      v[m] = pointwise_projection<Mode::kMod>(v[m], to_float(amp_tile[(t + T * m + rot) & (L - 1)]),
+                                              sc, acc, kHalfStorage<WT> ? 1.0f : sc);
     }
     // every line of the tile belongs to one start: one atomic per warp
     const double total = warp_sum_double(static_cast<double>(acc));

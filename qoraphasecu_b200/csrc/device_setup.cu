@@ -82,8 +82,9 @@ __global__ void threshold_kernel(const float* mag, long long n, const unsigned* 
 // Element e (FFT order) of one problem goes to index `tiled(e)` of the
 // signed-amplitude array: the modulus pass's CTA order for columns, element j
 // of line c of CTA tile t at (t * L + j) * lines + c (element-major, the
-// register-resident pass) or at (t * lines + c) * L + j (line-major, the TMA
-// column pass); FFT order otherwise.
+// register-resident pass) or at (t * lines + c) * L + (j + r_c) mod L
+// (line-major, the TMA column pass, r_c = amp_line_rotation(L, c)); FFT order
+// otherwise.
 __device__ __forceinline__ long long tiled_index(long long e, int L, int S, int lines,
                                                  bool line_major) {
   if (lines <= 0 || S == 1) return e;
@@ -93,7 +94,11 @@ __device__ __forceinline__ long long tiled_index(long long e, int L, int S, int 
   const long long j = rem / S;
   const long long col = rem - j * S;
   const long long tile = outer * (S / lines) + col / lines;
-  return line_major ? (tile * lines + col % lines) * L + j : (tile * L + j) * lines + col % lines;
+  if (line_major) {
+    const int line = static_cast<int>(col % lines);
+    return (tile * lines + line) * L + ((j + amp_line_rotation(L, line)) & (L - 1));
+  }
+  return (tile * L + j) * lines + col % lines;
 }
 
 template <class T>

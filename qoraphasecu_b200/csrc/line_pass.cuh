@@ -108,6 +108,16 @@ struct PassParams {
 inline constexpr int kAmpTiledElements = 1;
 inline constexpr int kAmpTiledLines = 2;
 
+// Line-major tiles (kAmpTiledLines) store line `line` of a tile rotated by
+// this many elements (element j at (j + rotation) mod L), so that the lines
+// one warp of a column tile reads (32 / T of them, T = the transform's
+// threads per line: L / 8 up to 64 points, L / 16 above) fall on disjoint
+// shared-memory banks.
+QPB_HD int amp_line_rotation(int L, int line) {
+  const int T = L <= 64 ? L / 8 : L / 16;
+  return T * (line % (32 / T));
+}
+
 // Element offset of the amplitude that global start `start` reads.
 QPB_HD long long amp_offset(const PassParams& p, int start) {
   return p.amp_stride ? static_cast<long long>(start / p.starts_per_problem) * p.amp_stride : 0;
