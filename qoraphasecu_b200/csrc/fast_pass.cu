@@ -78,7 +78,14 @@ struct Staging {
   static constexpr int kSideA = kAmp   ? G::LINES * L * static_cast<int>(sizeof(AmpT))
                                 : kUpd ? G::LINES * L * static_cast<int>(sizeof(XT))
                                        : 0;
-  static constexpr int kSideB = kUpd ? G::LINES * L : 0;
+  // The support tile's rows of up to 128 points sit L + 16 bytes apart (one
+  // bulk copy per row), which puts the 4 rows a warp reads on different banks:
+  // the 128^3 x-axis update pass went from 59.0 to 57.3 us. Rows of 256 keep
+  // one copy per tile (2 rows a warp, 2-way conflicts): a copy per row cost
+  // more there (11.26 -> 11.57 us for 32 starts of 256^2).
+  static constexpr int kSupportPitch = G::LINES > 1 && L <= 128 ? L + 16 : L;
+  static constexpr int kSupportBytes = G::LINES * L;  // bytes the copies deliver
+  static constexpr int kSideB = kUpd ? G::LINES * kSupportPitch : 0;
   static constexpr bool kBarrierUsed = kAmp || kUpd || kRowTma;
   static constexpr int kBarrier = align16(kExchange + kSideA + kSideB);
   static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : G::SMEM;
@@ -167,7 +174,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       if constexpr (St::kUpd) {
         mbar_arrive_expect_tx(bar, St::kTileIn);
         mbar_init(side_bar, 1);
-        mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSideB);
+        mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSupportBytes);
       } else {
         mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTileIn : 0) + St::kSideA + St::kSideB);
       }
@@ -185,7 +192,15 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       if (tid == 0 && !p.starve) {
         bulk_g2s(sbase + St::kExchange, reinterpret_cast<const XT*>(p.x) + line0 * L, St::kSideA,
                  side_bar);
-        bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSideB, side_bar);
+        if constexpr (St::kSupportPitch == L) {
+          bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSupportBytes,
+                   side_bar);
+        } else {
+          for (int r = 0; r < Ti::LINES; ++r) {
+            bulk_g2s(sbase + St::kExchange + St::kSideA + r * St::kSupportPitch,
+                     p.support + (line0 + r) * L, L, side_bar);
+          }
+        }
       }
     } else if constexpr (St::kAmp) {
       if (ROWS || p.amp_tiled) {
@@ -287,7 +302,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       for (int m = 0; m < E; ++m) {
         const int j = l * L + t + T * m;
         float2 xn = kHalfStorage<WT> ? cscale(v[m], p.scale) : v[m];
-        if (!s_tile[j]) {
+        if (!s_tile[l * St::kSupportPitch + t + T * m]) {
           const float2 xo = load_c(x_tile[j]);
           xn = {ca * xo.x + cb * xn.x, ca * xo.y + cb * xn.y};
         }
