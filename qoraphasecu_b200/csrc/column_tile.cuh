@@ -30,8 +30,9 @@ namespace qpb {
 // WT (float2 or __half2). A box row is LINES_ elements: 64 or 128 bytes of
 // complex64, 32 or 64 of fp16 pairs, swizzled with the pattern of that width.
 // The register budget is sized for MIN_CTAS resident CTAs per SM
-// (registers <= 64K / (NT * MIN_CTAS)): at 8 lines all CTAs of a 32-start
-// 256 x 256 launch fit in one wave.
+// (registers <= 64K / (NT * MIN_CTAS)): at 8 lines of 256 points, 5 CTAs per
+// SM leave the modulus tile 96 registers, enough to run without spills (7 per
+// SM spilled 32-40 bytes a thread and ran slower).
 template <int L, class WT, int LINES_>
 struct ColumnTiling {
   using G = Geometry<L>;
