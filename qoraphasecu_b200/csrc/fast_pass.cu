@@ -87,9 +87,15 @@ struct Staging {
   static constexpr int kSupportBytes = G::LINES * L;  // bytes the copies deliver
   static constexpr int kSideB = kUpd ? G::LINES * kSupportPitch : 0;
   static constexpr bool kBarrierUsed = kAmp || kUpd || kRowTma;
-  static constexpr int kBarrier = align16(kExchange + kSideA + kSideB);
+  // A row update (two transforms per tile) reads its twiddles from a copy of
+  // the stage-major table in shared memory, copied with the wave tile.
+  static constexpr bool kTwStaged = kUpd && Geometry<L>::STAGES > 1 && L <= 256;
+  static constexpr int kTwOffset = align16(kExchange + kSideA + kSideB);
+  static constexpr int kTwBytes = kTwStaged ? Geometry<L>::TW_COUNT * 8 : 0;
+  static constexpr int kBarrier = align16(kTwOffset + kTwBytes);
   static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : G::SMEM;
-  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTileIn % 16 == 0 && kTileOut % 16 == 0,
+  static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTileIn % 16 == 0 && kTileOut % 16 == 0 &&
+                    kTwBytes % 16 == 0,
                 "bulk copies need 16-byte sizes");
 };
 
@@ -130,7 +136,11 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   // modes that reach x or w by bulk copies or through one of them.
   WT* __restrict__ wl = reinterpret_cast<WT*>(p.w) + base;
   XT* __restrict__ xl = reinterpret_cast<XT*>(p.x) + base;
-  const float2* __restrict__ tw = p.stage_twiddle;
+  const float2* __restrict__ tw =
+      St::kTwStaged ? reinterpret_cast<const float2*>(reinterpret_cast<unsigned char*>(smem) +
+                                                      St::kTwOffset)
+                    : p.stage_twiddle;
+  constexpr bool kTwShared = St::kTwStaged;
   // A row's T threads share a warp, so its exchanges need warp barriers only.
   constexpr bool kWarpLocal = ROWS && T <= 32;
 
@@ -172,7 +182,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     if (tid == 0) {
       mbar_init(bar, 1);
       if constexpr (St::kUpd) {
-        mbar_arrive_expect_tx(bar, St::kTileIn);
+        mbar_arrive_expect_tx(bar, St::kTileIn + St::kTwBytes);
         mbar_init(side_bar, 1);
         mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSupportBytes);
       } else {
@@ -186,6 +196,9 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       if (tid == 0 && !p.starve) {
         const InT* src = reinterpret_cast<const InT*>(M == Mode::kFwdFromX ? p.x : p.w) + line0 * L;
         bulk_g2s(smem, src, St::kTileIn, bar);
+        if constexpr (St::kTwStaged) {
+          bulk_g2s(sbase + St::kTwOffset, p.stage_twiddle, St::kTwBytes, bar);
+        }
       }
     }
     if constexpr (St::kUpd) {
@@ -270,7 +283,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   // passes one in its error sum, an update in its store, and the passes of a
   // single transform only write the row again after the barrier below.
   constexpr bool kTrail = M == Mode::kBlur || M == Mode::kBlurMag;
-  transform<L, kStartsInverse, kWarpLocal, kTrail>(v, t, tw, row);
+  transform<L, kStartsInverse, kWarpLocal, kTrail, kTwShared>(v, t, tw, row);
 
   if constexpr (St::kAmp) {
     if (!staged(bar)) return;
@@ -291,7 +304,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     // exchange reads before the inverse's writes
     const double total = block_sum_double<false>(static_cast<double>(acc));
     if (tid == 0 && err_slot) atomicAdd(err_slot, total);
-    transform<L, true, kWarpLocal, false>(v, t, tw, row);
+    transform<L, true, kWarpLocal, false, kTwShared>(v, t, tw, row);
   } else if constexpr (M == Mode::kUpd) {
     if constexpr (St::kUpd) {
       if (!staged(side_bar)) return;
@@ -330,7 +343,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       __syncthreads();
     }
     if (p.bump_counter && blockIdx.x == 0 && tid == 0) ++p.ctrl->counters[p.group];
-    transform<L, false, kWarpLocal, false>(v, t, tw, row);
+    transform<L, false, kWarpLocal, false, kTwShared>(v, t, tw, row);
   } else if constexpr (M == Mode::kBlur || M == Mode::kBlurMag) {
     const float inv_l = 1.0f / static_cast<float>(L);
 #pragma unroll
