@@ -232,7 +232,7 @@ int column_pass_lines(const PassParams& p, Mode mode) {
 }
 
 bool column_pass_preferred(const PassParams& p, Mode mode) {
-  return p.L >= 256 && column_pass_lines(p, mode) > 0;
+  return p.L >= 128 && column_pass_lines(p, mode) > 0;
 }
 
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream) {

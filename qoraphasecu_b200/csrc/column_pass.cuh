@@ -20,11 +20,12 @@ bool column_passes_enabled();
 int column_pass_lines(const PassParams& p, Mode mode);
 
 // True where the TMA column pass is the one to run on this column axis: it can
-// (column_pass_lines) and its lines have 256 points. Lines of 64 and 128 points
-// run the register-resident column pass, which measured faster there (the
-// 128^3 crystal's z and y passes: 42.8 / 23.6 / 22.6 us against 45.7 / 25.2 /
-// 25.7 us); at 256 the TMA pass is faster (the 256^2 benchmark's modulus pass:
-// 14.2 against 14.6 us, its step 12.2 against 12.8 ms).
+// (column_pass_lines) and its lines have 128 or 256 points. At 256 it is the
+// faster pass (the 256^2 benchmark's modulus pass: 14.2 against 14.6 us, its
+// step 12.2 against 12.8 ms); at 128 the 128^3 crystal's whole iteration runs
+// 2.6% faster with it (36.6 k against 35.6 k start-iterations/s), although
+// its y-axis passes alone take about 2 us longer than the register-resident
+// ones. Lines of 64 points run the register-resident column pass.
 bool column_pass_preferred(const PassParams& p, Mode mode);
 
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream);
