@@ -69,7 +69,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // The launch's wave as a 3D tensor {S, L, outer slabs} of 8-byte (complex64)
-// or 4-byte (fp16 pair) elements and its [1][L][LINES] box.
+// or 4-byte (fp16 pair) elements and its [1][kBoxRows][LINES] box (a tile of
+// a line longer than 256 points takes several boxes).
 template <int L, class WT, int LINES>
 CUtensorMap wave_map(const PassParams& p) {
   using Ti = ColumnTiling<L, WT, LINES>;
@@ -79,7 +80,8 @@ CUtensorMap wave_map(const PassParams& p) {
                               static_cast<cuuint64_t>(p.lines / p.S)};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(p.S) * kElem,
                                  static_cast<cuuint64_t>(p.S) * L * kElem};
-  const cuuint32_t box[3] = {static_cast<cuuint32_t>(Ti::LINES), static_cast<cuuint32_t>(L), 1};
+  const cuuint32_t box[3] = {static_cast<cuuint32_t>(Ti::LINES),
+                             static_cast<cuuint32_t>(Ti::kBoxRows), 1};
   const cuuint32_t estrides[3] = {1, 1, 1};
   const CUresult r = encode_fn()(
       &map, kElem == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, p.w,
@@ -221,7 +223,7 @@ bool column_passes_enabled() {
 
 int column_pass_lines(const PassParams& p, Mode mode) {
   if (!column_passes_enabled() || p.S <= 1) return 0;
-  if (p.L != 64 && p.L != 128 && p.L != 256) return 0;
+  if (p.L != 64 && p.L != 128 && p.L != 256 && p.L != 512) return 0;
   if (mode != Mode::kMod && mode != Mode::kFwd && mode != Mode::kInv) return 0;
   if (mode == Mode::kMod && p.amp_tiled != kAmpTiledLines) return 0;
   constexpr int lines = kLines;
@@ -243,6 +245,8 @@ void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream) {
       return launch_length<128>(mode, p, stream);
     case 256:
       return launch_length<256>(mode, p, stream);
+    case 512:
+      return launch_length<512>(mode, p, stream);
     default:
       throw std::logic_error("column pass: unsupported length");
   }
@@ -258,6 +262,7 @@ void configure_column_passes() {
   allow_length<64>();
   allow_length<128>();
   allow_length<256>();
+  allow_length<512>();
 }
 
 }  // namespace qpb

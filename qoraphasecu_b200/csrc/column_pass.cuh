@@ -13,19 +13,20 @@ namespace qpb {
 bool column_passes_enabled();
 
 // Lines per CTA of the TMA column pass for `mode` with these parameters, or 0
-// when it does not take the pass: strided lines (S > 1) of 64, 128 or 256
+// when it does not take the pass: strided lines (S > 1) of 64, 128, 256 or 512
 // points, CTAs of 8 adjacent columns that never span two starts, modes kMod
 // (p.amp_tiled == kAmpTiledLines: the amplitude tiled line-major in this
 // pass's CTA order), kFwd and kInv.
 int column_pass_lines(const PassParams& p, Mode mode);
 
 // True where the TMA column pass is the one to run on this column axis: it can
-// (column_pass_lines) and its lines have 128 or 256 points. At 256 it is the
+// (column_pass_lines) and its lines have 128, 256 or 512 points. At 256 it is the
 // faster pass (the 256^2 benchmark's modulus pass: 14.2 against 14.6 us, its
 // step 12.2 against 12.8 ms); at 128 the 128^3 crystal's whole iteration runs
 // 2.6% faster with it (36.6 k against 35.6 k start-iterations/s), although
 // its y-axis passes alone take about 2 us longer than the register-resident
-// ones. Lines of 64 points run the register-resident column pass.
+// ones; at 512 its modulus pass takes 109 against 128 us (64 starts). Lines
+// of 64 points run the register-resident column pass.
 bool column_pass_preferred(const PassParams& p, Mode mode);
 
 void launch_column_pass(Mode mode, const PassParams& p, cudaStream_t stream);

@@ -38,9 +38,15 @@ struct ColumnTiling {
   using G = Geometry<L>;
   static constexpr int LINES = LINES_;
   static constexpr int NT = G::T * LINES;
-  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 5 : 3);
+  // (lines of 512 points: 256 threads and a three-stage transform, 2 CTAs per
+  // SM at up to 128 registers)
+  static constexpr int MIN_CTAS = NT <= 64 ? 12 : (NT <= 128 ? 5 : (L >= 512 ? 2 : 3));
   static constexpr int ROW_BYTES = LINES * static_cast<int>(sizeof(WT));  // one box row
   static constexpr int kBox = L * ROW_BYTES;
+  // A tensor-map box is at most 256 rows high: longer lines move in parts of
+  // kBoxRows rows, one copy each, to consecutive parts of the box.
+  static constexpr int kBoxRows = L < 256 ? L : 256;
+  static constexpr int kBoxParts = L / kBoxRows;
   // A half-warp holds 8 threads of each of two lines (column_tile_run); their
   // exchange rows sit 8 mod 16 complex values apart so that the two lines'
   // accesses fall on disjoint banks.
@@ -135,7 +141,11 @@ __device__ __forceinline__ void column_tile_issue(const CUtensorMap* wmap, const
   const int batch_start = static_cast<int>(line0 / p.lines_per_start);
   mbar_arrive_expect_tx(s.bar, St::kAmpBytes + (LOAD_TW ? St::kTwBytes : 0) + Ti::kBox);
   if (!p.starve) {
-    tma_load_3d(s.box, wmap, inner0, 0, outer, s.bar);
+#pragma unroll
+    for (int part = 0; part < Ti::kBoxParts; ++part) {
+      tma_load_3d(s.box + part * Ti::kBoxRows * Ti::ROW_BYTES, wmap, inner0, part * Ti::kBoxRows,
+                  outer, s.bar);
+    }
     if constexpr (LOAD_TW) {
       bulk_g2s(const_cast<float2*>(s.tw), p.stage_twiddle, St::kTwBytes, s.bar);
     }
@@ -231,7 +241,11 @@ __device__ __forceinline__ bool column_tile_run(const CUtensorMap* wmap, const P
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
-    tma_store_3d(wmap, inner0, 0, outer, s.box);
+#pragma unroll
+    for (int part = 0; part < Ti::kBoxParts; ++part) {
+      tma_store_3d(wmap, inner0, part * Ti::kBoxRows, outer,
+                   s.box + part * Ti::kBoxRows * Ti::ROW_BYTES);
+    }
     bulk_commit();
   }
   return true;

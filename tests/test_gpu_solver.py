@@ -65,6 +65,20 @@ def test_odd_and_3d_shapes_match_fp64(gpu, shape, m):
         np.testing.assert_array_equal(run.support, r_sup)
 
 
+@pytest.mark.parametrize("shape,m", [((512, 512), 40), ((256, 512), 30), ((512, 128), 24),
+                                     ((128, 128, 128), 16)])
+def test_tma_column_shapes_match_fp64(gpu, shape, m):
+    """Columns of 128, 256 and 512 points on the TMA column tiles (512-point
+    lines move as two boxes of 256 rows), with shrinkwrap between stages."""
+    _, support, intensity = triangle(shape, m)
+    recipe = Recipe(HIO(6), Shrinkwrap(), RAAR(4), ER(4))
+    ref, ours = run_both(intensity, support, recipe, starts=2, seed=4)
+    for (r_obj, r_sup, r_err), run in zip(ref, ours, strict=True):
+        np.testing.assert_allclose(run.errors, r_err, rtol=1e-4, atol=1e-7)
+        assert fp64.relative_diff(run.object, r_obj) < 1e-4
+        np.testing.assert_array_equal(run.support, r_sup)
+
+
 @pytest.mark.parametrize("variant", ["batched", "plain"])
 def test_given_start_matches_fp64(gpu, variant):
     """tests/test_cuda.cpp:104-119."""
