@@ -124,7 +124,7 @@ def to_centred(x, ndim):
 
 def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr: float = 1e-2,
                      seed: int | None = None, init=None, seconds: float | None = None,
-                     bound: float | None = 16.0, device: str = "cuda"):
+                     bound: float | None = 16.0, graph: bool = True, device: str = "cuda"):
     """Gradient-based reconstruction: Adam on the amplitude loss with the
     support projection after every step. Starts are drawn as ``Solver`` draws
     them (same seed -> same starting objects). Stops after ``steps`` steps or
@@ -145,7 +145,16 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
     ``bound`` caps every pixel's magnitude at ``bound`` times that RMS
     amplitude after each step (the projection onto a disc per pixel, which,
     like the support projection, leaves objects inside it unchanged); None
-    turns the cap off."""
+    turns the cap off.
+
+    With ``graph`` (the default) the first three steps run eagerly (on a side
+    stream, which also builds the optimiser's state and the library's plans)
+    and one step is then captured as a CUDA graph and replayed for the rest:
+    a step is about twenty small kernels whose launches from Python would
+    otherwise take longer than the work. The arithmetic is the same either
+    way (Adam runs with ``capturable=True`` in both), so the objects are
+    identical; only the FP64 sums of the per-step losses may differ in their
+    last bits."""
     torch = _torch()
     with Solver(problem, starts=starts, seed=seed, init=init) as drawn:
         first = drawn.results()
@@ -156,21 +165,42 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
     scale = float(np.sqrt(model.energy / inside)) or 1.0
     u = torch.from_numpy(x0 / np.float32(scale)).to(device).requires_grad_(True)
     support = model.support.to(torch.complex64)
-    opt = torch.optim.Adam([u], lr=lr)
-    history = []
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        opt.zero_grad(set_to_none=True)
+    opt = torch.optim.Adam([u], lr=lr, capturable=True)
+
+    def one_step():
         losses = amplitude_loss(u * scale, model)
         losses.sum().backward()
-        history.append(losses.detach())
         opt.step()
         with torch.no_grad():
             u.mul_(support)
             if bound is not None:
                 u.mul_(torch.clamp(bound / torch.abs(u).clamp_min(1e-30), max=1.0))
-        if seconds is not None and time.perf_counter() - t0 >= seconds:
-            break
+        return losses.detach()
+
+    def out_of_time():
+        return seconds is not None and time.perf_counter() - t0 >= seconds
+
+    history = []
+    t0 = time.perf_counter()
+    eager = min(steps, 3) if graph else steps
+    side = torch.cuda.Stream(device=u.device)
+    side.wait_stream(torch.cuda.current_stream(u.device))
+    with torch.cuda.stream(side):
+        for _ in range(eager):
+            opt.zero_grad(set_to_none=True)
+            history.append(one_step())
+            if out_of_time():
+                break
+    torch.cuda.current_stream(u.device).wait_stream(side)
+    if len(history) < steps and not out_of_time():
+        captured = torch.cuda.CUDAGraph()
+        opt.zero_grad(set_to_none=True)
+        with torch.cuda.graph(captured):
+            static_losses = one_step()
+        while len(history) < steps and not out_of_time():
+            captured.replay()
+            history.append(static_losses.clone())
+        del captured
     torch.cuda.synchronize()
     errors = torch.sqrt(torch.stack(history) / (model.energy + 1e-12)).to(torch.float32).cpu().numpy()
     final = to_centred(u.detach() * scale, ndim).cpu().numpy()

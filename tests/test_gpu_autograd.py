@@ -130,3 +130,16 @@ def test_adam_magnitude_bound_keeps_masked_directions_in_check(gpu):
         assert float(np.max(np.abs(b.object))) <= 8.0 * rms * (1 + 1e-5)
         assert np.all(b.object[~support.astype(bool)] == 0)
         assert b.errors[-1] <= f.errors[-1] * 1.25 + 1e-3
+
+
+def test_adam_graph_replay_equals_eager_steps(gpu):
+    """The captured step replays the eager step's arithmetic: identical
+    objects, per-step errors equal up to the FP64 sums' order."""
+    obj, support, intensity = triangle((64, 64), 20)
+    p = qpc.make_problem(intensity, support=support)
+    eager = qad.adam_reconstruct(p, starts=3, steps=40, lr=1e-2, seed=2, graph=False)
+    replayed = qad.adam_reconstruct(p, starts=3, steps=40, lr=1e-2, seed=2, graph=True)
+    for a, b in zip(eager, replayed, strict=True):
+        assert b.errors.shape == (40,)
+        np.testing.assert_array_equal(b.object, a.object)
+        np.testing.assert_allclose(b.errors, a.errors, rtol=1e-6)
