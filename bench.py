@@ -334,15 +334,26 @@ def parity_check(solver_kwargs, intensity, mask):
             "ok": bool(err < 1e-5 and obj < 1e-5)}
 
 
-def run_profile(iterations, schedule="streamed"):
+def run_profile(iterations, schedule="streamed", workload=None):
     """The benchmark workload cut to a few iterations, all 32 starts in one
     launch per pass and no autotuning, so that an ncu capture sees each line
     pass after a short set-up: make_problem, solver construction, `iterations`
-    RAAR iterations."""
+    RAAR iterations. With workload "crystal": the 128^3 crystal, its 4 starts
+    in one launch per pass, `iterations` HIO iterations."""
     import qoraphasecu_b200 as qpc
     from qoraphasecu_b200 import workloads
-    from qoraphasecu_b200.recipe import RAAR, Recipe
+    from qoraphasecu_b200.recipe import HIO, RAAR, Recipe
 
+    if workload == "crystal":
+        _, intensity = workloads.crystal(128, seed=3000)
+        problem = qpc.make_problem(intensity)
+        with qpc.Solver(problem, starts=4, seed=0, batch=4, schedule="streamed",
+                        sync_every=1) as solver:
+            solver.run(Recipe(HIO(iterations, 0.9)))
+            print(json.dumps({"profile_iterations": iterations, "workload": "crystal",
+                              "kernels": qpc.kernel_launches(),
+                              "final_errors": [float(r.error) for r in solver.results()]}))
+        return 0
     _, intensity, mask = workloads.gaussians(SHAPE[0], seed=SEED)
     problem = qpc.make_problem(intensity, mask=mask)
     if schedule == "resident":
@@ -593,7 +604,8 @@ def main(argv=None):
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     parser.add_argument("--no-extras", action="store_true", help="skip plain / f16 / e2e legs")
     parser.add_argument("--profile", type=int, default=0, metavar="ITERS",
-                        help="only build the workload and run ITERS RAAR iterations (for ncu)")
+                        help="only build the workload and run ITERS RAAR iterations (for ncu; "
+                             "with --workload crystal, ITERS HIO iterations of the 128^3 crystal)")
     parser.add_argument("--schedule", choices=("auto", "streamed", "resident"), default="auto",
                         help="batched schedule of the timed solver (auto = autotuned)")
     parser.add_argument("--workload", choices=sorted(WORKLOADS), default=None,
@@ -603,7 +615,8 @@ def main(argv=None):
                         help="only build the workload and run one benchmark step (for ncu)")
     args = parser.parse_args(argv)
     if args.profile:
-        return run_profile(args.profile, "resident" if args.schedule == "resident" else "streamed")
+        return run_profile(args.profile, "resident" if args.schedule == "resident" else "streamed",
+                           args.workload)
     if args.profile_step:
         return run_profile_step(args.sync_every, args.batch, args.schedule)
     if args.workload:
