@@ -59,7 +59,6 @@ struct Tiling {
   static constexpr int NT = G::T * LINES;
   static constexpr int MIN_CTAS = L >= 512 ? (NT < 512 ? 512 / NT : 1)
                                            : (NT <= 64 ? 12 : (NT <= 128 ? 6 : (NT <= 256 ? 3 : 1)));
-  static constexpr int SMEM = G::STAGES > 1 ? LINES * G::PITCH * 8 : 0;
 };
 
 // WT, XT: storage of the wave and of the iterate (float2 or __half2).
@@ -67,17 +66,33 @@ template <int L, bool ROWS, Mode M, class AmpT, class WT, class XT>
 struct Staging {
   using G = Tiling<L, ROWS>;
   using InT = std::conditional_t<M == Mode::kFwdFromX, XT, WT>;
-  static constexpr int kTileIn = G::LINES * L * static_cast<int>(sizeof(InT));
-  static constexpr int kTileOut = G::LINES * L * static_cast<int>(sizeof(WT));
-  static constexpr int kTile = kTileIn > kTileOut ? kTileIn : kTileOut;
   static constexpr bool kRowTma =
       ROWS && (M == Mode::kFwd || M == Mode::kFwdFromX || M == Mode::kInv || M == Mode::kUpd);
   static constexpr bool kAmp = M == Mode::kMod || M == Mode::kGrad;
   static constexpr bool kUpd = M == Mode::kUpd && ROWS;
-  static constexpr int kExchange = align16(kRowTma && kTile > G::SMEM ? kTile : G::SMEM);
+  // Rows of 128 points (8 threads a row, a half-warp holding two rows) sit
+  // kRowPitch elements apart in the staged wave, iterate and output tiles, one
+  // bulk copy per row, and the exchange rows kXPitch = 8 mod 16 values apart,
+  // so that the two rows of a half-warp fall on disjoint banks (rows L apart
+  // share them: the 128^3 x-axis update counted 2.3 M conflicts on 5.6 M
+  // shared-load wavefronts per launch of 4 starts).
+  static constexpr bool kPadRows = kRowTma && G::LINES > 1 && L == 128;
+  static constexpr int kRowPitch = kPadRows ? L + 8 : L;
+  static constexpr int kXPitch = kPadRows ? (Geometry<L>::PITCH + 7) / 16 * 16 + 8
+                                          : Geometry<L>::PITCH;
+  static constexpr int kTileIn = G::LINES * L * static_cast<int>(sizeof(InT));
+  static constexpr int kTileOut = G::LINES * L * static_cast<int>(sizeof(WT));
+  static constexpr int kTileSmem = G::LINES * kRowPitch *
+                                   static_cast<int>(sizeof(InT) > sizeof(WT) ? sizeof(InT)
+                                                                             : sizeof(WT));
+  static constexpr int kRowsSmem = Geometry<L>::STAGES > 1 ? G::LINES * kXPitch * 8 : 0;
+  static constexpr int kExchange =
+      align16(kRowTma && kTileSmem > kRowsSmem ? kTileSmem : kRowsSmem);
   static constexpr int kSideA = kAmp   ? G::LINES * L * static_cast<int>(sizeof(AmpT))
-                                : kUpd ? G::LINES * L * static_cast<int>(sizeof(XT))
+                                : kUpd ? G::LINES * kRowPitch * static_cast<int>(sizeof(XT))
                                        : 0;
+  static constexpr int kSideABytes =  // bytes the side-A copies deliver
+      kUpd ? G::LINES * L * static_cast<int>(sizeof(XT)) : kSideA;
   // The support tile's rows of up to 128 points sit L + 16 bytes apart (one
   // bulk copy per row), which puts the 4 rows a warp reads on different banks:
   // the 128^3 x-axis update pass went from 59.0 to 57.3 us. Rows of 256 keep
@@ -93,7 +108,7 @@ struct Staging {
   static constexpr int kTwOffset = align16(kExchange + kSideA + kSideB);
   static constexpr int kTwBytes = kTwStaged ? Geometry<L>::TW_COUNT * 8 : 0;
   static constexpr int kBarrier = align16(kTwOffset + kTwBytes);
-  static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : G::SMEM;
+  static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : kRowsSmem;
   static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTileIn % 16 == 0 && kTileOut % 16 == 0 &&
                     kTwBytes % 16 == 0,
                 "bulk copies need 16-byte sizes");
@@ -112,7 +127,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   const int tid = threadIdx.x;
   const int l = ROWS ? tid / T : tid % Ti::LINES;
   const int t = ROWS ? tid % T : tid / Ti::LINES;
-  float2* row = smem + l * G::PITCH;
+  float2* row = smem + l * St::kXPitch;
 
   const long long line0 = static_cast<long long>(blockIdx.x) * Ti::LINES;
   const int batch_start = static_cast<int>(line0 / p.lines_per_start);
@@ -184,7 +199,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       if constexpr (St::kUpd) {
         mbar_arrive_expect_tx(bar, St::kTileIn + St::kTwBytes);
         mbar_init(side_bar, 1);
-        mbar_arrive_expect_tx(side_bar, St::kSideA + St::kSupportBytes);
+        mbar_arrive_expect_tx(side_bar, St::kSideABytes + St::kSupportBytes);
       } else {
         mbar_arrive_expect_tx(bar, (St::kRowTma ? St::kTileIn : 0) + St::kSideA + St::kSideB);
       }
@@ -195,7 +210,14 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     if constexpr (St::kRowTma) {
       if (tid == 0 && !p.starve) {
         const InT* src = reinterpret_cast<const InT*>(M == Mode::kFwdFromX ? p.x : p.w) + line0 * L;
-        bulk_g2s(smem, src, St::kTileIn, bar);
+        if constexpr (St::kPadRows) {
+          for (int r = 0; r < Ti::LINES; ++r) {
+            bulk_g2s(reinterpret_cast<InT*>(smem) + r * St::kRowPitch, src + r * L,
+                     L * static_cast<int>(sizeof(InT)), bar);
+          }
+        } else {
+          bulk_g2s(smem, src, St::kTileIn, bar);
+        }
         if constexpr (St::kTwStaged) {
           bulk_g2s(sbase + St::kTwOffset, p.stage_twiddle, St::kTwBytes, bar);
         }
@@ -203,8 +225,15 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     }
     if constexpr (St::kUpd) {
       if (tid == 0 && !p.starve) {
-        bulk_g2s(sbase + St::kExchange, reinterpret_cast<const XT*>(p.x) + line0 * L, St::kSideA,
-                 side_bar);
+        const XT* xsrc = reinterpret_cast<const XT*>(p.x) + line0 * L;
+        if constexpr (St::kPadRows) {
+          for (int r = 0; r < Ti::LINES; ++r) {
+            bulk_g2s(reinterpret_cast<XT*>(sbase + St::kExchange) + r * St::kRowPitch,
+                     xsrc + r * L, L * static_cast<int>(sizeof(XT)), side_bar);
+          }
+        } else {
+          bulk_g2s(sbase + St::kExchange, xsrc, St::kSideA, side_bar);
+        }
         if constexpr (St::kSupportPitch == L) {
           bulk_g2s(sbase + St::kExchange + St::kSideA, p.support + line0 * L, St::kSupportBytes,
                    side_bar);
@@ -261,7 +290,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   if constexpr (St::kRowTma) {
     if (!staged(bar)) return;
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = load_c(in_tile[l * L + t + T * m]);
+    for (int m = 0; m < E; ++m) v[m] = load_c(in_tile[l * St::kRowPitch + t + T * m]);
     __syncthreads();  // region W becomes the exchange buffer
   } else {
 #pragma unroll
@@ -313,7 +342,7 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       const std::uint8_t* s_tile = sbase + St::kExchange + St::kSideA;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
-        const int j = l * L + t + T * m;
+        const int j = l * St::kRowPitch + t + T * m;
         float2 xn = kHalfStorage<WT> ? cscale(v[m], p.scale) : v[m];
         if (!s_tile[l * St::kSupportPitch + t + T * m]) {
           const float2 xo = load_c(x_tile[j]);
@@ -325,7 +354,14 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
       fence_proxy_async();
       __syncthreads();
       if (tid == 0) {
-        bulk_s2g(reinterpret_cast<XT*>(p.x) + line0 * L, x_tile, St::kSideA);
+        XT* xdst = reinterpret_cast<XT*>(p.x) + line0 * L;
+        if constexpr (St::kPadRows) {
+          for (int r = 0; r < Ti::LINES; ++r) {
+            bulk_s2g(xdst + r * L, x_tile + r * St::kRowPitch, L * static_cast<int>(sizeof(XT)));
+          }
+        } else {
+          bulk_s2g(xdst, x_tile, St::kSideA);
+        }
         bulk_commit();
       }
     } else {
@@ -360,11 +396,18 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
     // tile goes there and leaves by one bulk store.
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < E; ++m) out_tile[l * L + t + T * m] = store_c<WT>(v[m]);
+    for (int m = 0; m < E; ++m) out_tile[l * St::kRowPitch + t + T * m] = store_c<WT>(v[m]);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      bulk_s2g(reinterpret_cast<WT*>(p.w) + line0 * L, out_tile, St::kTileOut);
+      WT* wdst = reinterpret_cast<WT*>(p.w) + line0 * L;
+      if constexpr (St::kPadRows) {
+        for (int r = 0; r < Ti::LINES; ++r) {
+          bulk_s2g(wdst + r * L, out_tile + r * St::kRowPitch, L * static_cast<int>(sizeof(WT)));
+        }
+      } else {
+        bulk_s2g(wdst, out_tile, St::kTileOut);
+      }
       bulk_commit();
       bulk_wait_reads();
     }
