@@ -1,7 +1,8 @@
 // Column line passes (stride S > 1) whose tiles move by TMA: one tile of
 // column_tile.cuh per CTA (LINES adjacent columns as one [L][LINES] box of a
-// 3D tensor map over the launch's wave, {S, L, outer slabs}); this file holds
-// the kernel, the tensor-map encoding and the launch dispatch.
+// 3D tensor map over the launch's wave, {S, L, outer slabs}; lines of 512
+// points as two boxes of 256 rows); this file holds the kernel, the
+// tensor-map encoding and the launch dispatch.
 //
 // Every wait is bounded (PassParams::wait_tries); a CTA that gives up waits
 // once more for its copies in flight, counts itself in p.wait_failures and

@@ -31,9 +31,11 @@ __host__ __device__ constexpr int align16(int bytes) { return (bytes + 15) / 16 
 
 // Shared-memory layout of one CTA. Region W holds the Stockham exchange rows
 // and, for row passes that move whole tiles by bulk copies, the wave tile in
-// and out (its rows are contiguous in global memory); then the side inputs
-// staged by bulk copies (the amplitude tile of a modulus pass; the old-iterate
-// and support tiles of a row update); then two mbarriers (16 bytes).
+// and out (its rows are contiguous in global memory; rows of 128 points are
+// staged kRowPitch elements apart); then the side inputs staged by bulk
+// copies (the amplitude tile of a modulus pass; the old-iterate and support
+// tiles of a row update); then a row update's copy of the stage-major twiddle
+// table; then two mbarriers (16 bytes).
 // CTA shape of a streamed pass: lines per CTA, threads, the CTAs per SM the
 // register budget is sized for (registers <= 64K / (NT * MIN_CTAS)) and the
 // exchange rows. Rows of 256 points use 4 lines per CTA (64 threads, up to 12
