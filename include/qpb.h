@@ -256,7 +256,10 @@ QPB_API qpb_status qpb_tuning_report(char* out, size_t len);
  * *n_passes their count (<= 8; 2D: modulus pass, update pass; 3D adds the
  * y-axis inverse and forward passes). With the resident schedule, *n_passes =
  * 1 and ms_out[0] is the mean time per iteration of one launch running all
- * `iterations`. Changes the iterate. No counterpart in the reference: it
+ * `iterations`. Leaves the solver as it was: the passes run with ER
+ * coefficients, write no error rows and count no iterations, and the iterate
+ * and the wave are copied aside and back (one more copy of each on the device
+ * during the call). No counterpart in the reference: it
  * feeds the per-kernel roofline that bench.py reports. */
 QPB_API qpb_status qpb_profile_passes(qpb_solver* solver, int iterations, double* ms_out, int* n_passes);
 

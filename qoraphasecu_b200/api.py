@@ -451,7 +451,9 @@ class Solver:
         each pass launched ``iterations`` times back to back from one captured
         CUDA graph, whose replay two CUDA events time; with the resident
         schedule, one value: the mean time per iteration of one launch of
-        ``iterations`` iterations. Changes the iterate."""
+        ``iterations`` iterations. Leaves the solver as it was (iterate, wave,
+        error history and iteration count); the call holds one more copy of
+        the iterate and the wave on the device."""
         ms = (ctypes.c_double * 8)()
         n = ctypes.c_int()
         _lib.check(self._lib.qpb_profile_passes(self._handle, iterations, ms, ctypes.byref(n)))

@@ -299,3 +299,39 @@ def test_3d_register_passes_match_fp64(gpu, shape, m):
         np.testing.assert_allclose(run.errors, r_err, rtol=1e-4, atol=1e-7)
         assert fp64.relative_diff(run.object, r_obj) < 1e-4
         np.testing.assert_array_equal(run.support, r_sup)
+
+
+def test_profile_passes_times_every_pass(gpu):
+    """Each pass of an iteration is timed from a captured graph of launches:
+    two values in 2D, four in 3D, one for the resident kernel; on a caller's
+    stream too. The timing leaves the solver as it was: a run that profiles
+    between two recipes ends where the same run without the profile ends."""
+    import torch
+
+    _, support, intensity = triangle((64, 64), 20)
+    p2 = qpc.make_problem(intensity, support=support)
+    _, support3, intensity3 = triangle((32, 32, 32), 10)
+    p3 = qpc.make_problem(intensity3, support=support3)
+    stream = torch.cuda.Stream()
+    cases = [(p2, dict(schedule="streamed", batch=2), 2), (p3, dict(schedule="streamed", batch=2), 4),
+             (p2, dict(schedule="resident"), 1), (p2, dict(schedule="persistent"), 1),
+             (p2, dict(schedule="streamed", batch=4, stream=stream.cuda_stream), 2)]
+    for problem, kw, count in cases:
+        with qpc.Solver(problem, starts=4, seed=1, sync_every=5, **kw) as s:
+            s.run(Recipe(HIO(3)))
+            before = qpc.kernel_launches()
+            ms = s.profile_passes(4)
+            assert len(ms) == count
+            assert all(np.isfinite(m) and 0.0 < m < 10.0 for m in ms), ms
+            assert qpc.kernel_launches() > before
+            s.run(Recipe(ER(2)))
+            runs = s.results()
+        with qpc.Solver(problem, starts=4, seed=1, sync_every=5, **kw) as s:
+            s.run(Recipe(HIO(3)))
+            s.run(Recipe(ER(2)))
+            plain = s.results()
+        for r, q in zip(runs, plain, strict=True):
+            assert r.errors.shape == (5,)
+            assert np.all(np.isfinite(r.errors)) and np.all(r.errors > 0)
+            np.testing.assert_allclose(r.errors, q.errors, rtol=1e-6)
+            np.testing.assert_array_equal(r.object, q.object)
