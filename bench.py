@@ -747,7 +747,9 @@ def main(argv=None):
             "achieved_min_gbs": 21 * elems / (iter_ms * 1e6),
             "achieved_pass_gbs": fused_bytes / (iter_ms * 1e6),
         },
-        "note": "32 starts x 256^2 (16 MiB iterate) stay L2-resident across an iteration",
+        "note": "32 starts x 256^2 (16 MiB iterate) stay L2-resident across an iteration; "
+                "a launch of all 32 starts runs the modulus pass's 7-CTAs-per-SM variant "
+                "(the timed graph's 4-start launches run the default 5 per SM)",
         "passes_beyond_l2": beyond_l2,
     }
 

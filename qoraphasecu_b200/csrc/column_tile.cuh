@@ -31,8 +31,9 @@ namespace qpb {
 // complex64, 32 or 64 of fp16 pairs, swizzled with the pattern of that width.
 // The register budget is sized for MIN_CTAS resident CTAs per SM
 // (registers <= 64K / (NT * MIN_CTAS)): at 8 lines of 256 points, 5 CTAs per
-// SM leave the modulus tile 96 registers, enough to run without spills (7 per
-// SM spilled 32-40 bytes a thread and ran slower).
+// SM leave the modulus tile 96 registers (it uses 93). The column pass also
+// has a 7-per-SM variant of that tile (72 registers, no spills) for launches
+// larger than one wave.
 template <int L, class WT, int LINES_>
 struct ColumnTiling {
   using G = Geometry<L>;

@@ -4,8 +4,10 @@ The benchmark reconstructs the seeded ``gaussians`` problem (256 x 256, five
 Gaussian blobs with a smooth phase, Poisson counts at 1e6, beamstop of radius
 8 px, autocorrelation support) with 32 starts. Its timed solver runs streamed
 passes with 4 starts per launch as 8 parallel graph branches, the amplitude
-pre-tiled in the modulus pass's CTA order; the autotuner's other candidate is
-the resident cluster kernel. Both schedules are checked here from the
+pre-tiled in the modulus pass's CTA order; the autotuner's other candidates
+are the resident cluster kernel and larger launches (all 32 starts in one
+launch runs the modulus pass's 7-CTAs-per-SM variant). These schedules are
+checked here from the
 bit-identical random starts of the FP64 oracle (oracle/fp64.py, which restates
 the reference's CpuSolver, src/cpu/cpu_solver.cpp:82-93):
 
@@ -36,6 +38,9 @@ pytestmark = pytest.mark.gpu
 STARTS = 32
 SCHEDULES = {
     "streamed 4 per launch": dict(schedule="streamed", batch=4, sync_every=50),
+    # all 32 starts in one launch: 1024 CTAs of the modulus pass, more than one
+    # wave at its default occupancy, so its 7-CTAs-per-SM variant runs
+    "streamed 32 per launch": dict(schedule="streamed", batch=32, sync_every=50),
     "resident": dict(schedule="resident", sync_every=50),
 }
 
