@@ -112,7 +112,7 @@ struct Staging {
   static constexpr int kBarrier = align16(kTwOffset + kTwBytes);
   static constexpr int kBytes = kBarrierUsed ? kBarrier + 16 : kRowsSmem;
   static_assert(kSideA % 16 == 0 && kSideB % 16 == 0 && kTileIn % 16 == 0 && kTileOut % 16 == 0 &&
-                    kTwBytes % 16 == 0,
+                    kTwBytes % 16 == 0 && kSideABytes % 16 == 0 && kSupportBytes % 16 == 0,
                 "bulk copies need 16-byte sizes");
 };
 
