@@ -311,6 +311,19 @@ QPB_API qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int b
                                            const float* signed_amplitude, const float* x,
                                            float* grad, double* loss, void* stream);
 
+/* The projection after a gradient step (no counterpart in the reference; it
+ * follows qpb_support_project and adds a magnitude cap): for each of `batch`
+ * objects of `numel` complex64 elements in x (device memory, in place), an
+ * element outside the support (support[i] == 0; `support` is numel bytes of
+ * device memory, shared by the objects) becomes 0, and one inside whose
+ * magnitude exceeds `bound` is scaled onto the disc of radius `bound`; the
+ * others are left unchanged. bound = +infinity applies the support alone.
+ * Enqueued on `stream` (cudaStream_t; NULL = legacy default stream); returns
+ * without waiting. x must be 8-byte aligned, bound > 0, batch in
+ * [1, 65535]; otherwise QPB_INVALID_ARGUMENT. */
+QPB_API qpb_status qpb_project_support_bound(int64_t numel, int batch, const uint8_t* support,
+                                             float bound, float* x, void* stream);
+
 /* qpcu::aligned_error (include/qoraphasecu/metrics.hpp:12, src/core/metrics.cpp:17-86)
  * for `batch` candidates at once, on the device: out[b] = ||a_b - ref|| / ||ref||
  * after the best integer translation (cross-correlation peak), global phase and

@@ -60,6 +60,7 @@ EXPORTS = (
     "qpb_tuning_report",
     "qpb_profile_passes",
     "qpb_amplitude_loss_grad",
+    "qpb_project_support_bound",
     "qpb_modulus_project_noalloc",
     "qpb_aligned_error",
     "qpb_align",
@@ -164,6 +165,8 @@ def load():
         lib.qpb_modulus_project.argtypes = [POINTER(Problem), c_void_p, c_int, POINTER(c_float)]
         lib.qpb_amplitude_loss_grad.argtypes = [c_int, POINTER(c_int64), c_int, c_void_p,
                                                 c_void_p, c_void_p, c_void_p, c_void_p]
+        lib.qpb_project_support_bound.argtypes = [c_int64, c_int, c_void_p, c_float, c_void_p,
+                                                  c_void_p]
         lib.qpb_modulus_project_noalloc.argtypes = [c_int, POINTER(c_int64), c_void_p, c_void_p,
                                                     c_void_p, c_void_p, c_void_p, c_void_p]
         lib.qpb_support_project.argtypes = [c_void_p, c_void_p, c_size_t]

@@ -69,6 +69,29 @@ def _loss_and_grad(x, signed, shape):
     return loss, grad
 
 
+def project_support_bound(x, support, bound=None):
+    """In place on FFT-order objects x (complex64 CUDA tensor (..., *shape)):
+    0 outside ``support`` (bool CUDA tensor of the objects' shape), and inside
+    it every magnitude above ``bound`` scaled down onto ``bound`` (None: the
+    support alone). One pass of libqpb.so (``qpb_project_support_bound``) on
+    the current stream. Returns x."""
+    torch = _torch()
+    if not x.is_cuda or x.dtype != torch.complex64 or not x.is_contiguous():
+        raise ValueError("x must be a contiguous complex64 CUDA tensor")
+    if support.dtype != torch.bool or support.device != x.device or not support.is_contiguous():
+        raise ValueError("support must be a contiguous bool tensor on x's device")
+    numel = support.numel()
+    if tuple(x.shape[x.dim() - support.dim():]) != tuple(support.shape):
+        raise ValueError(f"x.shape {tuple(x.shape)} does not end with {tuple(support.shape)}")
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    _lib.check(lib.qpb_project_support_bound(
+        numel, x.numel() // numel, ctypes.c_void_p(support.data_ptr()),
+        float("inf") if bound is None else float(bound), ctypes.c_void_p(x.data_ptr()),
+        ctypes.c_void_p(stream)))
+    return x
+
+
 class AmplitudeLoss:
     """``AmplitudeLoss.apply(x, model)`` -> per-object losses (float64, shape (batch,))."""
 
@@ -169,7 +192,7 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
     # of about ten element-wise passes.
     w = torch.view_as_real(torch.from_numpy(x0 / np.float32(scale)).to(device)).clone()
     w.requires_grad_(True)
-    support = model.support.to(torch.float32).unsqueeze(-1)
+    support = model.support.contiguous()
     opt = torch.optim.Adam([w], lr=lr, capturable=True, fused=True)
 
     def one_step():
@@ -177,10 +200,7 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
         losses.sum().backward()
         opt.step()
         with torch.no_grad():
-            w.mul_(support)
-            if bound is not None:
-                magnitude = torch.abs(torch.view_as_complex(w))
-                w.mul_(torch.clamp(bound / magnitude.clamp_min(1e-30), max=1.0).unsqueeze(-1))
+            project_support_bound(torch.view_as_complex(w), support, bound)
         return losses.detach()
 
     def out_of_time():

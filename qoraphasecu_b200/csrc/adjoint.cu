@@ -8,6 +8,7 @@
 // forward transform, the gradient's point-wise step with the loss sum on the
 // outer axis, inverse transform.
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -100,7 +101,98 @@ void amplitude_loss_grad(int ndim, const long long* shape, int batch, const floa
   count_launches(1);
 }
 
+namespace {
+
+// One element of the projection after an optimiser step: 0 outside the
+// support; inside it, a magnitude above `bound` scaled down onto it.
+__device__ __forceinline__ float2 onto_support_and_disc(float2 v, unsigned char inside,
+                                                       float bound) {
+  if (!inside) return make_float2(0.0f, 0.0f);
+  const float m = hypotf(v.x, v.y);
+  if (m > bound) {
+    const float f = bound / m;
+    return make_float2(v.x * f, v.y * f);
+  }
+  return v;
+}
+
+// Two elements a thread per step (one 16-byte load and store), object
+// blockIdx.y; `pairs` = numel / 2 (numel even).
+__global__ void support_bound_pairs_kernel(float4* x, const uchar2* support, long long pairs,
+                                           float bound) {
+  float4* obj = x + static_cast<long long>(blockIdx.y) * pairs;
+  const long long step = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < pairs;
+       i += step) {
+    const float4 v = obj[i];
+    const uchar2 in = support[i];
+    const float2 a = onto_support_and_disc(make_float2(v.x, v.y), in.x, bound);
+    const float2 b = onto_support_and_disc(make_float2(v.z, v.w), in.y, bound);
+    obj[i] = make_float4(a.x, a.y, b.x, b.y);
+  }
+}
+
+// One element a thread per step (odd numel or x not 16-byte aligned).
+__global__ void support_bound_kernel(float2* x, const unsigned char* support, long long numel,
+                                     float bound) {
+  float2* obj = x + static_cast<long long>(blockIdx.y) * numel;
+  const long long step = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < numel;
+       i += step) {
+    obj[i] = onto_support_and_disc(obj[i], support[i], bound);
+  }
+}
+
+}  // namespace
+
+void project_support_bound(long long numel, int batch, const std::uint8_t* support, float bound,
+                           float2* x, cudaStream_t stream) {
+  if (numel < 1) throw InvalidArgument("numel must be >= 1");
+  if (batch < 1 || batch > 65535) throw InvalidArgument("batch must be in [1, 65535]");
+  if (!(bound > 0.0f)) throw InvalidArgument("bound must be > 0 (infinity: no bound)");
+  if (reinterpret_cast<std::uintptr_t>(x) % alignof(float2) != 0) {
+    throw InvalidArgument("qpb_project_support_bound: x must be 8-byte aligned");
+  }
+  // A grid-stride loop over each object, about 4 waves of 256-thread CTAs
+  // over all objects.
+  int device = 0;
+  int sms = 0;
+  QPB_CHECK(cudaGetDevice(&device));
+  QPB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const bool pairs = numel % 2 == 0 && reinterpret_cast<std::uintptr_t>(x) % 16 == 0 &&
+                     reinterpret_cast<std::uintptr_t>(support) % 2 == 0;
+  const long long items = pairs ? numel / 2 : numel;
+  const long long wanted = (items + 255) / 256;
+  const long long cap = std::max<long long>(1, 4LL * 8 * sms / batch);
+  const dim3 grid(static_cast<unsigned>(std::min(wanted, cap)), static_cast<unsigned>(batch));
+  if (pairs) {
+    support_bound_pairs_kernel<<<grid, 256, 0, stream>>>(
+        reinterpret_cast<float4*>(x), reinterpret_cast<const uchar2*>(support), items, bound);
+  } else {
+    support_bound_kernel<<<grid, 256, 0, stream>>>(x, support, numel, bound);
+  }
+  QPB_CHECK(cudaGetLastError());
+  count_launches(1);
+}
+
 }  // namespace qpb
+
+extern "C" qpb_status qpb_project_support_bound(int64_t numel, int batch, const uint8_t* support,
+                                                float bound, float* x, void* stream) {
+  try {
+    qpb::clear_last_error();
+    if (!support || !x) throw qpb::InvalidArgument("NULL argument");
+    qpb::project_support_bound(numel, batch, support, bound, reinterpret_cast<float2*>(x),
+                               static_cast<cudaStream_t>(stream));
+    return QPB_OK;
+  } catch (const std::invalid_argument& e) {
+    qpb::set_last_error(e.what());
+    return QPB_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    qpb::set_last_error(e.what());
+    return QPB_RUNTIME_ERROR;
+  }
+}
 
 extern "C" qpb_status qpb_amplitude_loss_grad(int ndim, const int64_t* shape, int batch,
                                               const float* signed_amplitude, const float* x,

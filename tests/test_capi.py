@@ -114,6 +114,22 @@ def test_metrics_validate_before_touching_a_device():
         qpc.aligned_error(a, np.zeros((4, 5), np.complex64))
 
 
+def test_support_bound_projection_validates_before_touching_a_device():
+    lib = _lib.load()
+    x = np.zeros(8, np.complex64)
+    s = np.ones(8, np.uint8)
+    args = (_lib.ptr(s),)
+    assert lib.qpb_project_support_bound(8, 1, *args, 0.0, _lib.ptr(x), None) == _lib.INVALID_ARGUMENT
+    assert lib.qpb_project_support_bound(8, 1, *args, float("nan"), _lib.ptr(x), None) == \
+        _lib.INVALID_ARGUMENT
+    assert lib.qpb_project_support_bound(0, 1, *args, 1.0, _lib.ptr(x), None) == _lib.INVALID_ARGUMENT
+    assert lib.qpb_project_support_bound(8, 0, *args, 1.0, _lib.ptr(x), None) == _lib.INVALID_ARGUMENT
+    assert lib.qpb_project_support_bound(8, 1, None, 1.0, _lib.ptr(x), None) == _lib.INVALID_ARGUMENT
+    misaligned = x.view(np.uint8)[4:].ctypes.data
+    assert lib.qpb_project_support_bound(4, 1, *args, 1.0, misaligned, None) == \
+        _lib.INVALID_ARGUMENT
+
+
 def test_run_rejects_null_solver_and_bad_recipes():
     lib = _lib.load()
     ops = (_lib.Op * 1)(_lib.Op(0, 0, 0, 0, 0, 0, 0))

@@ -143,3 +143,29 @@ def test_adam_graph_replay_equals_eager_steps(gpu):
         assert b.errors.shape == (40,)
         np.testing.assert_array_equal(b.object, a.object)
         np.testing.assert_allclose(b.errors, a.errors, rtol=1e-6)
+
+
+def test_project_support_bound_matches_the_elementwise_formula(gpu):
+    """The fused projection after an Adam step against the element-wise torch
+    formula it replaces (x * support, then x * min(1, bound / |x|)): two
+    elements a thread (even sizes) and one (odd sizes), batches of objects,
+    magnitudes on both sides of the bound, and the support alone."""
+    import torch
+
+    for shape, batch in (((64, 48), 3), ((15, 17), 2), ((8, 8, 9), 1)):
+        g = torch.Generator(device="cuda").manual_seed(5)
+        x = torch.randn((batch, *shape), dtype=torch.complex64, device="cuda", generator=g) * 4
+        support = torch.rand(shape, device="cuda", generator=g) > 0.3
+        inside = support.expand_as(x)
+        for bound in (3.0, None):
+            want = x * support
+            if bound is not None:
+                want = want * torch.clamp(bound / torch.abs(want).clamp_min(1e-30), max=1.0)
+            got = qad.project_support_bound(x.clone(), support, bound)
+            torch.testing.assert_close(got, want, rtol=1e-6, atol=0.0)
+            assert torch.all(got[~inside] == 0)
+            below = inside & (torch.abs(x) <= (bound if bound is not None else float("inf")))
+            assert torch.equal(got[below], x[below])
+            if bound is not None:
+                assert float(torch.abs(got).max()) <= bound * (1 + 1e-6)
+                assert bool(torch.any(~below & inside))  # some pixels were scaled
