@@ -49,6 +49,23 @@ class AmplitudeModel:
             np.ascontiguousarray(np.fft.ifftshift(problem.support) != 0)).to(device)
         self.energy = float(np.sum(np.where(mask != 0, 0.0, amp.astype(np.float64) ** 2)))
 
+    def scaled(self, scale: float) -> "AmplitudeModel":
+        """The model of objects measured in units of ``scale``: the amplitude
+        divided by it (masked pixels stay -1) and the energy by its square,
+        so that the loss of x / scale is the loss of x divided by scale^2."""
+        out = object.__new__(AmplitudeModel)
+        out.shape = self.shape
+        out.support = self.support
+        out.signed = _divide_usable(self.signed, scale)
+        out.energy = self.energy / (scale * scale)
+        return out
+
+
+def _divide_usable(signed, scale):
+    """The signed amplitude divided by ``scale`` on usable pixels (>= 0), -1 kept on masked ones."""
+    torch = _torch()
+    return torch.where(signed >= 0, signed / scale, signed).contiguous()
+
 
 def _loss_and_grad(x, signed, shape):
     torch = _torch()
@@ -195,8 +212,14 @@ def adam_reconstruct(problem: Problem, *, starts: int = 1, steps: int = 500, lr:
     support = model.support.contiguous()
     opt = torch.optim.Adam([w], lr=lr, capturable=True, fused=True)
 
+    # The loss of the objects x = w scale is scale^2 times the loss of w
+    # against the amplitude divided by scale: the passes run on w directly
+    # (no scaled copy of the objects forward, nor of the gradient backward).
+    model_w = model.scaled(scale)
+    squared = scale * scale
+
     def one_step():
-        losses = amplitude_loss(torch.view_as_complex(w) * scale, model)
+        losses = amplitude_loss(torch.view_as_complex(w), model_w) * squared
         losses.sum().backward()
         opt.step()
         with torch.no_grad():
