@@ -25,6 +25,7 @@
 
 #include "column_pass.cuh"
 #include "column_tile.cuh"
+#include "dependent_launch.cuh"
 
 namespace qpb {
 
@@ -63,6 +64,8 @@ __global__ void __launch_bounds__(ColumnTiling<L, WT, LINES_>::NT, CTAS)
   s.err_slot = reinterpret_cast<double**>(sbase + St::kBarrier + 8);
   if (threadIdx.x == 0) mbar_init(s.bar, 1);
   __syncthreads();  // the barrier is initialised before anyone polls it
+  wait_for_prior_kernel();  // the wave and the control block come from it
+  allow_next_kernel();
   if (column_tile<L, M, AmpT, WT, LINES_, true>(&wmap, p, blockIdx.x, s, 0, -1)) {
     if (threadIdx.x == 0) bulk_wait_reads();
   }
@@ -159,14 +162,14 @@ void launch_lines(const PassParams& p, cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(ctas));
   if constexpr (kHasWide<L, M, WT>) {
     if (ctas > static_cast<long long>(Ti::MIN_CTAS) * device_sms()) {
-      column_pass_kernel<L, M, AmpT, WT, LINES, kWideCtas><<<grid, Ti::NT, kBytes, stream>>>(map, p);
-      QPB_CHECK(cudaGetLastError());
+      launch_dependent(column_pass_kernel<L, M, AmpT, WT, LINES, kWideCtas>, grid, dim3(Ti::NT),
+                       kBytes, stream, map, p);
       count_launches(1);
       return;
     }
   }
-  column_pass_kernel<L, M, AmpT, WT, LINES, Ti::MIN_CTAS><<<grid, Ti::NT, kBytes, stream>>>(map, p);
-  QPB_CHECK(cudaGetLastError());
+  launch_dependent(column_pass_kernel<L, M, AmpT, WT, LINES, Ti::MIN_CTAS>, grid, dim3(Ti::NT),
+                   kBytes, stream, map, p);
   count_launches(1);
 }
 

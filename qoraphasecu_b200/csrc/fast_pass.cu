@@ -17,6 +17,7 @@
 #include <stdexcept>
 
 #include "bulk_copy.cuh"
+#include "dependent_launch.cuh"
 #include "fast_pass.cuh"
 #include "line_fft.cuh"
 #include "projection.cuh"
@@ -130,6 +131,8 @@ __global__ void __launch_bounds__(Tiling<L, ROWS>::NT, Tiling<L, ROWS>::MIN_CTAS
   const int l = ROWS ? tid / T : tid % Ti::LINES;
   const int t = ROWS ? tid % T : tid / Ti::LINES;
   float2* row = smem + l * St::kXPitch;
+  wait_for_prior_kernel();  // its wave, iterate, support and control block
+  allow_next_kernel();
 
   const long long line0 = static_cast<long long>(blockIdx.x) * Ti::LINES;
   const int batch_start = static_cast<int>(line0 / p.lines_per_start);
@@ -451,9 +454,8 @@ template <int L, bool ROWS, Mode M, class AmpT, class WT, class XT>
 void launch_one(const PassParams& p, cudaStream_t stream) {
   using Ti = Tiling<L, ROWS>;
   const dim3 grid(static_cast<unsigned>(p.lines / Ti::LINES));
-  fast_pass_kernel<L, ROWS, M, AmpT, WT, XT>
-      <<<grid, Ti::NT, Staging<L, ROWS, M, AmpT, WT, XT>::kBytes, stream>>>(p);
-  QPB_CHECK(cudaGetLastError());
+  launch_dependent(fast_pass_kernel<L, ROWS, M, AmpT, WT, XT>, grid, dim3(Ti::NT),
+                   Staging<L, ROWS, M, AmpT, WT, XT>::kBytes, stream, p);
   count_launches(1);
 }
 
