@@ -186,6 +186,70 @@ def adjoint_512(full):
             "gradient_rel_l2_vs_2(x-P_M x)": fp64.relative_diff(g, identity)}
 
 
+def _adam_fp64(x0, scale, amp, usable, support, steps, lr, bound):
+    """The Adam reconstruction of qoraphasecu_b200.autograd.adam_reconstruct
+    in FP64 on the host (torch, complex128, torch.fft in place of the line
+    passes): Adam on the real view of w = x / scale, the loss
+    sum_usable (|F x| - A)^2 with F the unitary FFT, then the support
+    projection and the magnitude bound. Returns the objects x (FFT order) and
+    the Fourier error sqrt(loss / energy) of every step."""
+    import torch
+
+    w = torch.view_as_real(torch.from_numpy(x0 / scale)).clone().requires_grad_(True)
+    opt = torch.optim.Adam([w], lr=lr)
+    amp_t = torch.from_numpy(amp)
+    usable_t = torch.from_numpy(usable.astype(np.float64))
+    support_t = torch.from_numpy(support.astype(np.float64))
+    energy = float(np.sum(np.where(usable, amp ** 2, 0.0)))
+    errors = []
+    for _ in range(steps):
+        opt.zero_grad()
+        y = torch.fft.fft2(torch.view_as_complex(w) * scale, norm="ortho")
+        loss = (((torch.abs(y) - amp_t) ** 2) * usable_t).sum(dim=(-2, -1))
+        loss.sum().backward()
+        opt.step()
+        with torch.no_grad():
+            u = torch.view_as_complex(w)
+            u.mul_(support_t)
+            u.mul_(torch.clamp(bound / torch.abs(u).clamp_min(1e-300), max=1.0))
+        errors.append(np.sqrt(loss.detach().numpy() / energy))
+    x = (torch.view_as_complex(w.detach()) * scale).numpy()
+    return x, np.stack(errors, axis=1)
+
+
+def adam_512(full):
+    """Config 4's optimisation itself: adam_reconstruct (FP32 line passes,
+    torch's fused Adam on the real view, the fused support-and-bound
+    projection, graph replay) against the same algorithm in FP64, from the
+    same starts."""
+    rng = np.random.default_rng(4000)
+    obj = workloads.square(512, seed=4000)
+    intensity = workloads.poisson(workloads.simulate_intensity(obj), 1e7, rng)
+    mask = workloads.beamstop((512, 512), 12)
+    p = qpc.make_problem(intensity, mask=mask)
+    starts, lr, bound = 2, 1e-2, 16.0
+    out = {"workload": "square 512x512 (box 192), Poisson 1e7, beamstop 12: Adam(lr 1e-2), "
+                       "support projection, bound 16, 2 starts, FP32 against FP64"}
+    with qpc.Solver(p, starts=starts, seed=0) as drawn:
+        first = drawn.results()
+    x0 = np.stack([np.fft.ifftshift(r.object) for r in first]).astype(np.complex128)
+    amp = np.fft.ifftshift(np.asarray(p.amplitude, np.float64))
+    usable = np.fft.ifftshift(np.asarray(p.mask)) == 0
+    support = np.fft.ifftshift(np.asarray(p.support)) != 0
+    energy = float(np.sum(np.where(usable, amp ** 2, 0.0)))
+    scale = float(np.sqrt(energy / max(int(support.sum()), 1))) or 1.0
+    for steps in (20, 200) if full else (20, 100):
+        ours = qad.adam_reconstruct(p, starts=starts, steps=steps, lr=lr, seed=0, bound=bound)
+        x, errors = _adam_fp64(x0, scale, amp, usable, support, steps, lr, bound)
+        err = max(float(np.max(np.abs(r.errors - e) / e)) for r, e in zip(ours, errors))
+        obj_diff = max(fp64.relative_diff(r.object, np.fft.fftshift(xs))
+                       for r, xs in zip(ours, x))
+        out[f"steps_{steps}"] = {"error_rel_max": err, "object_rel_l2_max": obj_diff,
+                                 "final_error_fp32": [float(r.errors[-1]) for r in ours],
+                                 "final_error_fp64": [float(e[-1]) for e in errors]}
+    return out
+
+
 def crystal_128(full):
     obj, intensity = workloads.crystal(128, seed=3000)
     support = qpc.autocorrelation_support(intensity)
@@ -194,7 +258,7 @@ def crystal_128(full):
 
 
 REPORTS = {"square": square_64, "gaussians": gaussians_256, "uneven": uneven,
-           "adjoint": adjoint_512, "crystal": crystal_128}
+           "adjoint": adjoint_512, "adam": adam_512, "crystal": crystal_128}
 
 
 def main(argv=None):
